@@ -1,0 +1,200 @@
+/*
+ * nbx.h -- C ABI of the B200 Barnes-Hut + collision step.
+ *
+ * A drop-in for the per-step path of tyreecepaul/n-body-simulation:
+ * Simulation::step = iterate -> collide -> attract (src/Simulation.cpp:11-16,
+ * src/cuda/CudaSimulation.cu:51-58).  Plain C types only; every call returns
+ * an nbx_status and never exits the process (the reference's CUDA_CHECK
+ * aborts, src/cuda/DeviceBodies.cuh:18-27).  One handle = one CUDA stream
+ * and its captured step graphs; handles are independent (no global state),
+ * a handle must not be used from two threads at once.
+ *
+ * A handle holds one or more independent simulations ("instances") of fixed
+ * sizes, advanced together: one instance is the reference's Simulation /
+ * CudaSimulation; many is the batched ensemble.
+ */
+#ifndef NBX_H
+#define NBX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes. */
+typedef enum nbx_status {
+  NBX_OK = 0,
+  NBX_ERR_ARG = 1,         /* bad argument or size mismatch */
+  NBX_ERR_CUDA = 2,        /* a CUDA call failed (see nbx_last_error) */
+  NBX_ERR_CAPACITY = 3,    /* tree-node or collision-pair capacity exceeded */
+  NBX_ERR_NONFINITE = 4,   /* a body position became NaN or infinite */
+  NBX_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
+  NBX_ERR_STATE = 6,       /* call not valid in the handle's state */
+  NBX_ERR_NOMEM = 7        /* device or host allocation failed */
+} nbx_status;
+
+/* Same 36-byte layout as the reference's Body (src/Body.h:5-13):
+ * pos, vel, acc (Vec2 = 2 floats each), mass, radius, id. */
+typedef struct nbx_body {
+  float pos_x, pos_y;
+  float vel_x, vel_y;
+  float acc_x, acc_y;
+  float mass;
+  float radius;
+  uint32_t id;
+} nbx_body;
+
+/* Step parameters.  Defaults (nbx_params_default) are the reference's:
+ * dt 0.05 (Simulation.cpp:8), theta 1, epsilon 1, leaf capacity 16
+ * (Simulation.cpp:9, TreeKernels.cuh:32-34), collisions on
+ * (CudaSimulation.cuh:39-42). */
+typedef struct nbx_params {
+  float dt;
+  float theta;
+  float epsilon;
+  int32_t leaf_capacity;  /* 1..64 */
+  int32_t collisions;     /* 0/1 */
+  int32_t exact_math;     /* 1: force arithmetic exactly as the reference
+                             writes it (no FMA contraction, IEEE reciprocal),
+                             bit-identical to the CPU traversal on the same
+                             tree; 0: contracted, hardware reciprocal */
+  int32_t use_mlp;        /* 1: learned far-field correction (nbx_mlp_*) */
+  float node_factor;      /* node capacity per body (default 8, the
+                             reference bound 8n+8, CudaQuadTree.cu:270-273) */
+  float pair_factor;      /* collision partner slots per body (default 32) */
+  int32_t force_blocks;   /* 0 = auto; else blocks of the force launch */
+} nbx_params;
+
+typedef struct nbx_handle nbx_handle;
+
+/* Step phases for nbx_phase (the reference's Simulation::iterate/collide/
+ * attract and CudaQuadTree::build/computeForces, CudaSimulation.cuh:34-37,
+ * CudaQuadTree.cuh:26-32). */
+typedef enum nbx_phase_id {
+  NBX_PHASE_ITERATE = 0,
+  NBX_PHASE_COLLIDE = 1,
+  NBX_PHASE_BUILD = 2,   /* bounds, Morton codes, sort, permute, tree */
+  NBX_PHASE_FORCES = 3,  /* traversal of the last built tree */
+  NBX_PHASE_ATTRACT = 4, /* BUILD then FORCES */
+  NBX_PHASE_STEP = 5     /* ITERATE, COLLIDE (if on), ATTRACT */
+} nbx_phase_id;
+
+/* Fills p with the reference defaults.  (Simulation.cpp:7-9) */
+int nbx_params_default(nbx_params *p);
+
+/* Creates a handle on the current CUDA device for `num_instances`
+ * instances of the given sizes (bodies are laid out instance after
+ * instance).  Replaces `CudaSimulation(n)` / `CudaQuadTree(n)` /
+ * `CudaCollider(b)` construction (CudaSimulation.cu:34-38,
+ * CudaQuadTree.cu:269-334). */
+int nbx_create(const nbx_params *p, uint32_t num_instances,
+               const uint32_t *instance_sizes, nbx_handle **out);
+
+/* Releases every device allocation of the handle. */
+int nbx_destroy(nbx_handle *h);
+
+/* Parameters; takes effect at the next step (graphs are re-captured).
+ * Replaces the public fields dt/theta/epsilon/collisions of CudaSimulation
+ * (CudaSimulation.cuh:39-42) and QuadTree(theta, epsilon, leafCapacity)
+ * (QuadTree.h:76-79). */
+int nbx_set_params(nbx_handle *h, const nbx_params *p);
+int nbx_get_params(const nbx_handle *h, nbx_params *p);
+
+/* Bodies in and out, 36-byte Body records, all instances back to back.
+ * Replaces DeviceBodies::upload/download (DeviceBodies.cu:25-72).  Upload
+ * also fixes each instance's collision cell from its radii (CudaCollision.cu
+ * :201-215).  id_order = 1 writes body with id k of instance j at
+ * instance_start(j) + k (Main.cpp:55-62 sortById); it requires the ids of
+ * each instance to be a permutation of 0..size-1. */
+int nbx_upload_bodies(nbx_handle *h, const nbx_body *bodies, size_t n);
+int nbx_download_bodies(nbx_handle *h, nbx_body *bodies, size_t n,
+                        int id_order);
+
+/* Advances every instance by `steps` Simulation::step()s
+ * (Simulation.cpp:11-16).  Asynchronous: launches the captured step graph
+ * per step and returns; errors raised on the device surface at nbx_sync. */
+int nbx_step(nbx_handle *h, uint32_t steps);
+
+/* Waits for the handle's stream and reports (and clears) device-side
+ * error bits: NBX_ERR_CAPACITY, NBX_ERR_NONFINITE, NBX_ERR_TIMEOUT. */
+int nbx_sync(nbx_handle *h);
+
+/* Runs one phase eagerly (no graph); for parity checks. */
+int nbx_phase(nbx_handle *h, int phase);
+
+/* --- introspection of the last build / collide (parity checks) --- */
+
+/* Morton codes of the last build in pre-sort body order, and the sort
+ * permutation (sorted position -> pre-sort index), instance-local values.
+ * (CudaQuadTree.cu:400-407) */
+int nbx_get_morton(nbx_handle *h, uint32_t instance, uint64_t *codes,
+                   uint32_t *perm, size_t n);
+
+/* Node count and level count of an instance's last tree
+ * (CudaQuadTree::nodeCount/levelCount, CudaQuadTree.cuh:34-36). */
+int nbx_tree_size(nbx_handle *h, uint32_t instance, uint32_t *node_count,
+                  uint32_t *level_count);
+
+/* Node arrays of the last tree in the reference's breadth-first layout
+ * (TreeKernels.cuh:88-95, CudaQuadTree::download CudaQuadTree.cu:515-533);
+ * each array holds node_count entries; any pointer may be NULL. */
+int nbx_get_tree(nbx_handle *h, uint32_t instance, float *com_x, float *com_y,
+                 float *mass, float *center_x, float *center_y, float *size,
+                 int32_t *children, int32_t *next, int32_t *start,
+                 int32_t *end, size_t capacity);
+
+/* Candidate pairs of the last collide in resolution (pairLess) order,
+ * (later, earlier) body indices in the pre-collide order
+ * (Collision.cpp:333-348).  *count receives the pair total; nothing is
+ * written past `capacity`. */
+int nbx_get_pairs(nbx_handle *h, int32_t *later, int32_t *earlier,
+                  int64_t capacity, int64_t *count);
+
+/* --- FP64 checks --- */
+
+/* FP64 direct-sum accelerations with the tree's force law (no softening
+ * change, eps = params.epsilon) for bodies at the given current indices
+ * (exactTreeLawForces, CheckCuda.cu:453-475). */
+int nbx_direct_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m,
+                    double *ax, double *ay);
+
+/* Relative force error of the last force pass against nbx_direct_fp64 for
+ * the given targets: stats = {median, p99, max, mean}; per-target errors
+ * are written to err if not NULL.  (CheckCuda.cu:580-625) */
+int nbx_force_error_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m,
+                         double *stats, double *err);
+
+/* Compensated FP64 sums over all bodies: {kinetic energy, px, py, Lz,
+ * total mass}.  No counterpart in the reference. */
+int nbx_energy_momentum_fp64(nbx_handle *h, double *out5);
+
+/* Device status bits (cleared on read) and the last error message. */
+int nbx_status_bits(nbx_handle *h, uint32_t *bits);
+const char *nbx_last_error(const nbx_handle *h);
+
+/* --- host-side scenario generators (product host code) --- */
+
+/* uniformDisc(n, seed): src/Utils.cpp:6-54. */
+int nbx_uniform_disc(uint32_t n, uint32_t seed, nbx_body *out);
+
+/* Two discs of n/2 and n - n/2 bodies (seeds seed, seed+1) centred at
+ * (-sep/2, 0) and (+sep/2, 0) with sep = 6R (R = 5*sqrt(n/2), the disc
+ * radius), bulk velocities (0, -f*v) and (0, +f*v) with
+ * v = sqrt(M_total / (6R)), the second disc's spin reversed, ids renumbered
+ * 0..n-1 (after viewer/Scenarios.cpp:36-48). */
+int nbx_two_discs(uint32_t n, uint32_t seed, float approach_fraction,
+                  nbx_body *out);
+
+/* n unit-mass, radius-1 bodies at rest uniform in [-h, h]^2 with
+ * h = 3*sqrt(n), mt19937(seed) (viewer/Scenarios.cpp:50-57). */
+int nbx_cold_square(uint32_t n, uint32_t seed, nbx_body *out);
+
+/* Library build/version string. */
+const char *nbx_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NBX_H */

@@ -1,0 +1,758 @@
+// api.cu -- the C ABI (include/nbx.h): handles, device memory, step
+// sequencing and graph capture, introspection for parity checks.
+#include "nbx.h"
+#include "nbx_state.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace nbx {
+void launch_integrate(cudaStream_t s, const DevState &S, bool integrate,
+                      bool collide);
+void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
+                    SortScratch &sort);
+void launch_bounds(cudaStream_t s, const DevState &S);
+void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
+                  SortScratch &sort);
+void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks);
+void launch_direct_fp64(cudaStream_t s, const float4 *pv, const float2 *mr,
+                        uint32_t n, const uint32_t *targets, uint32_t m,
+                        double eps, double2 *partial, double *ax, double *ay);
+size_t direct_partial_elems(uint32_t m);
+void launch_energy_momentum(cudaStream_t s, const float4 *pv, const float2 *mr,
+                            uint32_t n, double *part, double *out);
+} // namespace nbx
+
+using namespace nbx;
+
+namespace {
+
+__global__ void k_unpack(const nbx_body *__restrict__ in, uint32_t n,
+                         float4 *pv, float2 *acc, float2 *mr, uint32_t *id) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    const nbx_body b = in[i];
+    pv[i] = make_float4(b.pos_x, b.pos_y, b.vel_x, b.vel_y);
+    acc[i] = make_float2(b.acc_x, b.acc_y);
+    mr[i] = make_float2(b.mass, b.radius);
+    id[i] = b.id;
+  }
+}
+
+// Body records; id_order scatters body i to instance_start + id.
+__global__ void k_pack(const float4 *__restrict__ pv, const float2 *__restrict__ acc,
+                       const float2 *__restrict__ mr, const uint32_t *__restrict__ id,
+                       const uint16_t *__restrict__ segOf, const SegDev *seg,
+                       uint32_t n, int idOrder, nbx_body *out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    const float4 p = pv[i];
+    const float2 a = acc[i];
+    const float2 m = mr[i];
+    nbx_body b;
+    b.pos_x = p.x;
+    b.pos_y = p.y;
+    b.vel_x = p.z;
+    b.vel_y = p.w;
+    b.acc_x = a.x;
+    b.acc_y = a.y;
+    b.mass = m.x;
+    b.radius = m.y;
+    b.id = id[i];
+    const uint32_t dst = idOrder ? seg[segOf[i]].start + b.id : i;
+    out[dst] = b;
+  }
+}
+
+__global__ void k_fill_u16(uint16_t *p, uint32_t start, uint32_t count,
+                           uint16_t v) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += gridDim.x * blockDim.x)
+    p[start + i] = v;
+}
+
+template <typename T> struct DevBuf {
+  T *p = nullptr;
+  size_t n = 0;
+};
+
+} // namespace
+
+struct nbx_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  nbx_params params{};
+  uint32_t n = 0, nseg = 0;
+  std::vector<uint32_t> segStart, segCount;
+  std::vector<void *> allocs;
+  DevState base{};       // buffer set A current
+  int cur = 0;           // 0: state in set A (pv), 1: in set B (pv2)
+  ScanScratch scan;
+  SortScratch sort;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  bool graphsValid = false;
+  bool uploaded = false;
+  bool treeValid = false;
+  bool collideValid = false;
+  bool idsPermutation = false;
+  nbx_body *dAoS = nullptr;     // device staging of body records
+  nbx_body *hPinned = nullptr;  // pinned host staging
+  double2 *dPartial = nullptr;  // FP64 direct-sum partials
+  uint32_t dPartialTargets = 0;
+  double *dF64 = nullptr;       // small FP64 scratch
+  uint32_t *dTargets = nullptr;
+  std::string lastError;
+
+  DevState state() const {
+    DevState S = base;
+    if (cur == 1) {
+      std::swap(S.pv, S.pv2);
+      std::swap(S.mr, S.mr2);
+      std::swap(S.id, S.id2);
+    }
+    return S;
+  }
+};
+
+namespace {
+
+int fail(nbx_handle *h, int code, const std::string &msg) {
+  if (h) h->lastError = msg;
+  return code;
+}
+
+int cuda_fail(nbx_handle *h, cudaError_t e, const char *what) {
+  if (h) {
+    h->lastError = std::string(what) + ": " + cudaGetErrorString(e);
+  }
+  return e == cudaErrorMemoryAllocation ? NBX_ERR_NOMEM : NBX_ERR_CUDA;
+}
+
+#define NBX_CUDA(h, call)                                                    \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess) return cuda_fail((h), e_, #call);                 \
+  } while (0)
+
+template <typename T> cudaError_t dalloc(nbx_handle *h, T *&p, size_t count) {
+  void *v = nullptr;
+  const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(&v, bytes);
+  if (e != cudaSuccess) return e;
+  h->allocs.push_back(v);
+  p = static_cast<T *>(v);
+  return cudaMemset(v, 0, bytes);
+}
+
+uint32_t next_pow2(uint64_t v) {
+  uint64_t p = 1;
+  while (p < v) p <<= 1;
+  return (uint32_t)std::min<uint64_t>(p, 1ull << 31);
+}
+
+int allocate(nbx_handle *h) {
+  DevState &S = h->base;
+  const uint32_t n = h->n, ns = h->nseg;
+  const nbx_params &P = h->params;
+  S.n = n;
+  S.nseg = ns;
+  const double nf = P.node_factor > 0 ? P.node_factor : 8.0f;
+  S.nodeCapacity = (uint32_t)std::min<double>(nf * n + 8.0 * ns + 8, 2.0e9);
+  const double pf = P.pair_factor > 0 ? P.pair_factor : 32.0f;
+  S.pairCapacity = (uint32_t)std::min<double>(pf * n + 64, 2.0e9);
+  S.nBuckets = next_pow2(2ull * std::max<uint32_t>(n, 1));
+  const uint32_t nodes = S.nodeCapacity;
+  const uint32_t sortCap = 2 * n + 64;
+#define A(ptr, count) \
+  if (cudaError_t e = dalloc(h, ptr, count)) return cuda_fail(h, e, "cudaMalloc " #ptr)
+  A(S.seg, ns);
+  A(S.segOf, n);
+  A(S.pv, n);
+  A(S.mr, n);
+  A(S.id, n);
+  A(S.pv2, n);
+  A(S.mr2, n);
+  A(S.id2, n);
+  A(S.acc, n);
+  A(S.xym, n);
+  A(S.bounds, 4 * ns);
+  A(S.status, 1);
+  A(S.box, n);
+  A(S.cellXY, n);
+  A(S.slot, n);
+  A(S.bucketCount, S.nBuckets + 1);
+  A(S.bucketStart, S.nBuckets + 2);
+  A(S.grid, n);
+  A(S.largeCount, ns);
+  A(S.largeStartA, ns + 1);
+  A(S.largeList, n);
+  A(S.deg, n);
+  A(S.pstart, n + 1);
+  A(S.plist, S.pairCapacity);
+  A(S.plistTmp, S.pairCapacity);
+  A(S.fillLarge, n);
+  A(S.nLater, n);
+  A(S.unitFlag, n);
+  A(S.unitPos, n + 1);
+  A(S.prog, n);
+  A(S.unitOrder, n);
+  A(S.counters, 16);
+  A(S.codes, n);
+  A(S.perm, n);
+  A(S.sortedCodes, n);
+  A(S.splitCount, n);
+  A(S.splitStart, n + 1);
+  A(S.splitLo, n);
+  A(S.groupStart, (size_t)ns * kLevelSlots);
+  A(S.groupEnd, (size_t)ns * kLevelSlots);
+  A(S.levelStart, (size_t)ns * (kLevelSlots + 1));
+  A(S.comX, nodes);
+  A(S.comY, nodes);
+  A(S.mass, nodes);
+  A(S.centerX, nodes);
+  A(S.centerY, nodes);
+  A(S.size, nodes);
+  A(S.children, nodes);
+  A(S.next, nodes);
+  A(S.start, nodes);
+  A(S.end, nodes);
+  A(S.parent, nodes);
+  A(S.sumX, nodes);
+  A(S.sumY, nodes);
+  A(S.moments, nodes);
+  A(S.subtree, nodes);
+  A(S.arrive, nodes);
+  A(S.tA, nodes);
+  A(S.tB, nodes);
+  A(S.tM, nodes);
+  // scan / sort scratch
+  SortScratch &so = h->sort;
+  so.capacity = sortCap;
+  so.maxTiles = (uint32_t)sort_tiles(sortCap);
+  A(so.keys[0], sortCap);
+  A(so.keys[1], sortCap);
+  A(so.vals[0], sortCap);
+  A(so.vals[1], sortCap);
+  A(so.hist, 8 * 256);
+  A(so.status, (size_t)so.maxTiles * 256 + 256);
+  A(so.tileCounter, 8);
+  ScanScratch &sc = h->scan;
+  sc.maxTiles = (uint32_t)scan_scratch_tiles(std::max<uint32_t>(S.nBuckets + 2, sortCap));
+  A(sc.status, sc.maxTiles + 1);
+  A(sc.tileCounter, 1);
+  A(h->dAoS, n);
+  A(h->dF64, 16 * 592);
+#undef A
+  // bounds accumulators start empty
+  std::vector<uint32_t> b(4 * ns);
+  for (uint32_t s = 0; s < ns; ++s) {
+    b[4 * s + 0] = 0xffffffffu;
+    b[4 * s + 1] = 0u;
+    b[4 * s + 2] = 0xffffffffu;
+    b[4 * s + 3] = 0u;
+  }
+  NBX_CUDA(h, cudaMemcpy(S.bounds, b.data(), b.size() * 4, cudaMemcpyHostToDevice));
+  // instance table and body -> instance map
+  std::vector<SegDev> seg(ns);
+  for (uint32_t s = 0; s < ns; ++s) {
+    std::memset(&seg[s], 0, sizeof(SegDev));
+    seg[s].start = h->segStart[s];
+    seg[s].count = h->segCount[s];
+    seg[s].cell = 1.0f;
+    seg[s].invCell = 1.0f;
+    seg[s].smallW = 0.999f;
+  }
+  NBX_CUDA(h, cudaMemcpy(S.seg, seg.data(), ns * sizeof(SegDev), cudaMemcpyHostToDevice));
+  for (uint32_t s = 0; s < ns; ++s) {
+    if (h->segCount[s] == 0) continue;
+    k_fill_u16<<<256, 256, 0, h->stream>>>(S.segOf, h->segStart[s], h->segCount[s],
+                                          (uint16_t)s);
+  }
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  NBX_CUDA(h, cudaMallocHost(&h->hPinned, std::max<size_t>(n, 1) * sizeof(nbx_body)));
+  return NBX_OK;
+}
+
+void sync_params(nbx_handle *h) {
+  DevState &S = h->base;
+  const nbx_params &P = h->params;
+  S.dt = P.dt;
+  S.tSq = P.theta * P.theta;
+  S.eSq = P.epsilon * P.epsilon;
+  S.leafCapacity = P.leaf_capacity;
+  S.collisions = P.collisions;
+}
+
+// One Simulation::step on stream s for state S; returns the state after the
+// Morton gather's buffer swap.
+DevState enqueue_step(nbx_handle *h, cudaStream_t s, DevState S) {
+  if (S.collisions) {
+    cudaMemsetAsync(S.bucketCount, 0, sizeof(uint32_t) * (S.nBuckets + 1), s);
+    cudaMemsetAsync(S.largeCount, 0, sizeof(uint32_t) * S.nseg, s);
+  }
+  launch_integrate(s, S, true, S.collisions != 0);
+  if (S.collisions) launch_collide(s, S, h->scan, h->sort);
+  launch_build(s, S, h->scan, h->sort);
+  launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks);
+  return S;
+}
+
+void destroy_graphs(nbx_handle *h) {
+  for (auto &g : h->graph) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+  h->graphsValid = false;
+}
+
+int capture_graphs(nbx_handle *h) {
+  destroy_graphs(h);
+  for (int p = 0; p < 2; ++p) {
+    const int saved = h->cur;
+    h->cur = p;
+    const DevState S = h->state();
+    h->cur = saved;
+    cudaGraph_t g = nullptr;
+    NBX_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(h, h->stream, S);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&h->graph[p], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+  }
+  h->graphsValid = true;
+  return NBX_OK;
+}
+
+int check_status(nbx_handle *h) {
+  uint32_t bits = 0;
+  NBX_CUDA(h, cudaMemcpyAsync(&bits, h->base.status, 4, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (!bits) return NBX_OK;
+  NBX_CUDA(h, cudaMemsetAsync(h->base.status, 0, 4, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (bits & kStatusSpinLimit) return fail(h, NBX_ERR_TIMEOUT, "a bounded device wait gave up");
+  if (bits & (kStatusTreeCapacity | kStatusPairCapacity | kStatusLargeCapacity))
+    return fail(h, NBX_ERR_CAPACITY, bits & kStatusTreeCapacity
+                                         ? "tree node capacity exceeded"
+                                         : "collision pair capacity exceeded");
+  if (bits & kStatusNonFinite) return fail(h, NBX_ERR_NONFINITE, "non-finite body position");
+  return fail(h, NBX_ERR_STATE, "device status bits set");
+}
+
+bool valid_params(const nbx_params *p) {
+  return p && p->dt == p->dt && p->theta >= 0.0f && p->epsilon >= 0.0f &&
+         p->leaf_capacity >= 1 && p->leaf_capacity <= 64;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *nbx_version(void) { return "nbx 0.1 (sm_100a)"; }
+
+int nbx_params_default(nbx_params *p) {
+  if (!p) return NBX_ERR_ARG;
+  std::memset(p, 0, sizeof(*p));
+  p->dt = 0.05f;
+  p->theta = 1.0f;
+  p->epsilon = 1.0f;
+  p->leaf_capacity = 16;
+  p->collisions = 1;
+  p->exact_math = 0;
+  p->use_mlp = 0;
+  p->node_factor = 8.0f;
+  p->pair_factor = 32.0f;
+  p->force_blocks = 0;
+  return NBX_OK;
+}
+
+int nbx_create(const nbx_params *p, uint32_t num, const uint32_t *sizes,
+               nbx_handle **out) {
+  if (!out || num == 0 || !sizes || num > 65535) return NBX_ERR_ARG;
+  *out = nullptr;
+  nbx_params P;
+  nbx_params_default(&P);
+  if (p) P = *p;
+  if (!valid_params(&P)) return NBX_ERR_ARG;
+  uint64_t total = 0;
+  for (uint32_t s = 0; s < num; ++s) total += sizes[s];
+  if (total >= (1ull << 30)) return NBX_ERR_ARG;
+  nbx_handle *h = new (std::nothrow) nbx_handle();
+  if (!h) return NBX_ERR_NOMEM;
+  h->params = P;
+  h->n = (uint32_t)total;
+  h->nseg = num;
+  uint32_t run = 0;
+  for (uint32_t s = 0; s < num; ++s) {
+    h->segStart.push_back(run);
+    h->segCount.push_back(sizes[s]);
+    run += sizes[s];
+  }
+  cudaError_t e = cudaGetDevice(&h->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  int rc = e == cudaSuccess ? allocate(h) : cuda_fail(h, e, "stream");
+  if (rc != NBX_OK) {
+    std::fprintf(stderr, "nbx_create: %s\n", h->lastError.c_str());
+    nbx_destroy(h);
+    return rc;
+  }
+  sync_params(h);
+  *out = h;
+  return NBX_OK;
+}
+
+int nbx_destroy(nbx_handle *h) {
+  if (!h) return NBX_ERR_ARG;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  destroy_graphs(h);
+  for (void *v : h->allocs) cudaFree(v);
+  if (h->hPinned) cudaFreeHost(h->hPinned);
+  if (h->dPartial) cudaFree(h->dPartial);
+  if (h->dTargets) cudaFree(h->dTargets);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return NBX_OK;
+}
+
+int nbx_set_params(nbx_handle *h, const nbx_params *p) {
+  if (!h || !valid_params(p)) return NBX_ERR_ARG;
+  const bool sizes = p->node_factor != h->params.node_factor ||
+                     p->pair_factor != h->params.pair_factor;
+  if (sizes) return fail(h, NBX_ERR_ARG, "capacity factors are fixed at nbx_create");
+  h->params = *p;
+  sync_params(h);
+  destroy_graphs(h);
+  return NBX_OK;
+}
+
+int nbx_get_params(const nbx_handle *h, nbx_params *p) {
+  if (!h || !p) return NBX_ERR_ARG;
+  *p = h->params;
+  return NBX_OK;
+}
+
+int nbx_upload_bodies(nbx_handle *h, const nbx_body *bodies, size_t n) {
+  if (!h || (!bodies && n) || n != h->n) return h ? fail(h, NBX_ERR_ARG, "body count mismatch") : NBX_ERR_ARG;
+  if (n == 0) {
+    h->uploaded = true;
+    return NBX_OK;
+  }
+  cudaPointerAttributes attr{};
+  const bool pinned = cudaPointerGetAttributes(&attr, bodies) == cudaSuccess &&
+                      attr.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  const void *src = bodies;
+  if (!pinned) {
+    std::memcpy(h->hPinned, bodies, n * sizeof(nbx_body));
+    src = h->hPinned;
+  }
+  NBX_CUDA(h, cudaMemcpyAsync(h->dAoS, src, n * sizeof(nbx_body),
+                              cudaMemcpyHostToDevice, h->stream));
+  const DevState S = h->state();
+  k_unpack<<<std::min<uint32_t>((h->n + 255) / 256, 4096), 256, 0, h->stream>>>(
+      h->dAoS, h->n, S.pv, S.acc, S.mr, S.id);
+  NBX_CUDA(h, cudaGetLastError());
+  // collision cell per instance: 2 x median radius x 1.01 (CudaCollision.cu:201-215)
+  std::vector<SegDev> seg(h->nseg);
+  NBX_CUDA(h, cudaMemcpyAsync(seg.data(), S.seg, h->nseg * sizeof(SegDev),
+                              cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  bool perm = true;
+  std::vector<float> radii;
+  std::vector<uint8_t> seen;
+  for (uint32_t s = 0; s < h->nseg; ++s) {
+    const uint32_t s0 = h->segStart[s], cnt = h->segCount[s];
+    radii.resize(cnt);
+    seen.assign(cnt, 0);
+    for (uint32_t i = 0; i < cnt; ++i) {
+      radii[i] = bodies[s0 + i].radius;
+      const uint32_t id = bodies[s0 + i].id;
+      if (id >= cnt || seen[id]) perm = false;
+      else seen[id] = 1;
+    }
+    float cell = 1.0f;
+    if (cnt) {
+      std::nth_element(radii.begin(), radii.begin() + cnt / 2, radii.end());
+      cell = 2.0f * radii[cnt / 2] * 1.01f;
+    }
+    if (!(cell > 0.0f) || !std::isfinite(cell)) cell = 1.0f;
+    seg[s].cell = cell;
+    seg[s].invCell = 1.0f / cell;
+    seg[s].smallW = cell * 0.999f;
+  }
+  NBX_CUDA(h, cudaMemcpyAsync(S.seg, seg.data(), h->nseg * sizeof(SegDev),
+                              cudaMemcpyHostToDevice, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->idsPermutation = perm;
+  h->uploaded = true;
+  h->treeValid = false;
+  h->collideValid = false;
+  return NBX_OK;
+}
+
+int nbx_download_bodies(nbx_handle *h, nbx_body *bodies, size_t n, int idOrder) {
+  if (!h || (!bodies && n) || n != h->n) return h ? fail(h, NBX_ERR_ARG, "body count mismatch") : NBX_ERR_ARG;
+  if (idOrder && !h->idsPermutation)
+    return fail(h, NBX_ERR_ARG, "ids are not a permutation of 0..size-1 per instance");
+  if (n == 0) return NBX_OK;
+  const DevState S = h->state();
+  k_pack<<<std::min<uint32_t>((h->n + 255) / 256, 4096), 256, 0, h->stream>>>(
+      S.pv, S.acc, S.mr, S.id, S.segOf, S.seg, h->n, idOrder, h->dAoS);
+  NBX_CUDA(h, cudaGetLastError());
+  cudaPointerAttributes attr{};
+  const bool pinned = cudaPointerGetAttributes(&attr, bodies) == cudaSuccess &&
+                      attr.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  void *dst = pinned ? (void *)bodies : (void *)h->hPinned;
+  NBX_CUDA(h, cudaMemcpyAsync(dst, h->dAoS, n * sizeof(nbx_body),
+                              cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (!pinned) std::memcpy(bodies, h->hPinned, n * sizeof(nbx_body));
+  return check_status(h);
+}
+
+int nbx_step(nbx_handle *h, uint32_t steps) {
+  if (!h) return NBX_ERR_ARG;
+  if (!h->uploaded) return fail(h, NBX_ERR_STATE, "no bodies uploaded");
+  if (h->n == 0 || steps == 0) return NBX_OK;
+  if (!h->graphsValid) {
+    int rc = capture_graphs(h);
+    if (rc != NBX_OK) return rc;
+  }
+  for (uint32_t k = 0; k < steps; ++k) {
+    NBX_CUDA(h, cudaGraphLaunch(h->graph[h->cur], h->stream));
+    h->cur ^= 1;
+  }
+  h->treeValid = true;
+  h->collideValid = h->params.collisions != 0;
+  return NBX_OK;
+}
+
+int nbx_sync(nbx_handle *h) {
+  if (!h) return NBX_ERR_ARG;
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  return check_status(h);
+}
+
+int nbx_phase(nbx_handle *h, int phase) {
+  if (!h) return NBX_ERR_ARG;
+  if (!h->uploaded) return fail(h, NBX_ERR_STATE, "no bodies uploaded");
+  if (h->n == 0) return NBX_OK;
+  cudaStream_t s = h->stream;
+  DevState S = h->state();
+  switch (phase) {
+  case NBX_PHASE_ITERATE:
+    launch_integrate(s, S, true, false);
+    break;
+  case NBX_PHASE_COLLIDE:
+    cudaMemsetAsync(S.bucketCount, 0, sizeof(uint32_t) * (S.nBuckets + 1), s);
+    cudaMemsetAsync(S.largeCount, 0, sizeof(uint32_t) * S.nseg, s);
+    launch_integrate(s, S, false, true);
+    launch_collide(s, S, h->scan, h->sort);
+    h->collideValid = true;
+    break;
+  case NBX_PHASE_BUILD:
+    launch_build(s, S, h->scan, h->sort);
+    h->cur ^= 1;
+    h->treeValid = true;
+    break;
+  case NBX_PHASE_FORCES:
+    if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
+    launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks);
+    break;
+  case NBX_PHASE_ATTRACT:
+    launch_build(s, S, h->scan, h->sort);
+    h->cur ^= 1;
+    h->treeValid = true;
+    launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks);
+    break;
+  case NBX_PHASE_STEP:
+    enqueue_step(h, s, S);
+    h->cur ^= 1;
+    h->treeValid = true;
+    h->collideValid = S.collisions != 0;
+    break;
+  default:
+    return fail(h, NBX_ERR_ARG, "unknown phase");
+  }
+  NBX_CUDA(h, cudaGetLastError());
+  return nbx_sync(h);
+}
+
+int nbx_get_morton(nbx_handle *h, uint32_t inst, uint64_t *codes, uint32_t *perm,
+                   size_t n) {
+  if (!h || inst >= h->nseg || n != h->segCount[inst]) return NBX_ERR_ARG;
+  if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
+  const uint32_t s0 = h->segStart[inst];
+  if (codes)
+    NBX_CUDA(h, cudaMemcpyAsync(codes, h->base.codes + s0, n * 8, cudaMemcpyDeviceToHost, h->stream));
+  std::vector<uint32_t> p(n);
+  NBX_CUDA(h, cudaMemcpyAsync(p.data(), h->base.perm + s0, n * 4, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (perm)
+    for (size_t i = 0; i < n; ++i) perm[i] = p[i] - s0;
+  return NBX_OK;
+}
+
+static int read_seg(nbx_handle *h, uint32_t inst, SegDev &g) {
+  NBX_CUDA(h, cudaMemcpyAsync(&g, h->base.seg + inst, sizeof(SegDev),
+                              cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  return NBX_OK;
+}
+
+int nbx_tree_size(nbx_handle *h, uint32_t inst, uint32_t *nodes, uint32_t *levels) {
+  if (!h || inst >= h->nseg) return NBX_ERR_ARG;
+  if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
+  SegDev g;
+  int rc = read_seg(h, inst, g);
+  if (rc) return rc;
+  if (nodes) *nodes = g.nodeCount;
+  if (levels) *levels = g.levelCount;
+  return NBX_OK;
+}
+
+int nbx_get_tree(nbx_handle *h, uint32_t inst, float *comX, float *comY, float *mass,
+                 float *cx, float *cy, float *size, int32_t *children, int32_t *next,
+                 int32_t *start, int32_t *end, size_t capacity) {
+  if (!h || inst >= h->nseg) return NBX_ERR_ARG;
+  if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
+  SegDev g;
+  int rc = read_seg(h, inst, g);
+  if (rc) return rc;
+  if (capacity < g.nodeCount) return fail(h, NBX_ERR_ARG, "capacity below node count");
+  const size_t c = g.nodeCount, b = g.nodeBase;
+  const DevState &S = h->base;
+  struct {
+    void *dst;
+    const void *src;
+  } arrays[] = {{comX, S.comX}, {comY, S.comY}, {mass, S.mass}, {cx, S.centerX},
+                {cy, S.centerY}, {size, S.size}, {children, S.children},
+                {next, S.next}, {start, S.start}, {end, S.end}};
+  for (auto &a : arrays) {
+    if (!a.dst || !c) continue;
+    NBX_CUDA(h, cudaMemcpyAsync(a.dst, (const char *)a.src + b * 4, c * 4,
+                                cudaMemcpyDeviceToHost, h->stream));
+  }
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  return NBX_OK;
+}
+
+int nbx_get_pairs(nbx_handle *h, int32_t *later, int32_t *earlier, int64_t cap,
+                  int64_t *count) {
+  if (!h || !count) return NBX_ERR_ARG;
+  if (!h->collideValid) return fail(h, NBX_ERR_STATE, "no collide run");
+  const DevState &S = h->base;
+  const uint32_t n = h->n;
+  uint32_t cnt[2];
+  NBX_CUDA(h, cudaMemcpyAsync(cnt, S.counters, 8, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  const uint32_t total = cnt[0], units = cnt[1];
+  if (total > S.pairCapacity) return fail(h, NBX_ERR_CAPACITY, "pair capacity exceeded");
+  std::vector<uint32_t> pstart(n), plist(total), nl(n), order(units);
+  NBX_CUDA(h, cudaMemcpyAsync(pstart.data(), S.pstart, 4ull * n, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaMemcpyAsync(plist.data(), S.plist, 4ull * total, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaMemcpyAsync(nl.data(), S.nLater, 4ull * n, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaMemcpyAsync(order.data(), S.unitOrder, 4ull * units, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  int64_t k = 0;
+  for (uint32_t u = 0; u < units; ++u) {
+    const uint32_t L = order[u];
+    for (uint32_t j = 0; j < nl[L]; ++j, ++k) {
+      if (k < cap) {
+        later[k] = (int32_t)L;
+        earlier[k] = (int32_t)plist[pstart[L] + j];
+      }
+    }
+  }
+  *count = k;
+  return NBX_OK;
+}
+
+int nbx_direct_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m, double *ax,
+                    double *ay) {
+  if (!h || (m && (!targets || !ax || !ay))) return NBX_ERR_ARG;
+  if (m == 0) return NBX_OK;
+  for (uint32_t k = 0; k < m; ++k)
+    if (targets[k] >= h->n) return fail(h, NBX_ERR_ARG, "target index out of range");
+  if (h->dPartialTargets < m) {
+    if (h->dPartial) cudaFree(h->dPartial);
+    if (h->dTargets) cudaFree(h->dTargets);
+    h->dPartial = nullptr;
+    h->dTargets = nullptr;
+    h->dPartialTargets = 0;
+    NBX_CUDA(h, cudaMalloc(&h->dPartial, direct_partial_elems(m) * sizeof(double2) + 16 * m));
+    NBX_CUDA(h, cudaMalloc(&h->dTargets, 4ull * m));
+    h->dPartialTargets = m;
+  }
+  double *dOut = reinterpret_cast<double *>(h->dPartial + direct_partial_elems(h->dPartialTargets));
+  NBX_CUDA(h, cudaMemcpyAsync(h->dTargets, targets, 4ull * m, cudaMemcpyHostToDevice, h->stream));
+  const DevState S = h->state();
+  launch_direct_fp64(h->stream, S.pv, S.mr, h->n, h->dTargets, m, h->params.epsilon,
+                     h->dPartial, dOut, dOut + m);
+  NBX_CUDA(h, cudaGetLastError());
+  NBX_CUDA(h, cudaMemcpyAsync(ax, dOut, 8ull * m, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaMemcpyAsync(ay, dOut + m, 8ull * m, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  return NBX_OK;
+}
+
+int nbx_force_error_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m,
+                         double *stats, double *err) {
+  if (!h || !stats) return NBX_ERR_ARG;
+  std::vector<double> ex(m), ey(m);
+  int rc = nbx_direct_fp64(h, targets, m, ex.data(), ey.data());
+  if (rc) return rc;
+  const DevState S = h->state();
+  std::vector<float2> acc(h->n);
+  NBX_CUDA(h, cudaMemcpyAsync(acc.data(), S.acc, 8ull * h->n, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::vector<double> e(m);
+  double mean = 0.0;
+  for (uint32_t k = 0; k < m; ++k) {
+    const float2 a = acc[targets[k]];
+    const double dx = (double)a.x - ex[k], dy = (double)a.y - ey[k];
+    const double ref = std::sqrt(ex[k] * ex[k] + ey[k] * ey[k]);
+    e[k] = std::sqrt(dx * dx + dy * dy) / std::max(ref, 1e-30);
+    mean += e[k];
+    if (err) err[k] = e[k];
+  }
+  std::vector<double> s = e;
+  std::sort(s.begin(), s.end());
+  stats[0] = m ? s[m / 2] : 0.0;
+  stats[1] = m ? s[std::min<size_t>(m - 1, (size_t)(0.99 * m))] : 0.0;
+  stats[2] = m ? s.back() : 0.0;
+  stats[3] = m ? mean / m : 0.0;
+  return NBX_OK;
+}
+
+int nbx_energy_momentum_fp64(nbx_handle *h, double *out5) {
+  if (!h || !out5) return NBX_ERR_ARG;
+  const DevState S = h->state();
+  launch_energy_momentum(h->stream, S.pv, S.mr, h->n, h->dF64, h->dF64 + 10 * 592);
+  NBX_CUDA(h, cudaGetLastError());
+  NBX_CUDA(h, cudaMemcpyAsync(out5, h->dF64 + 10 * 592, 40, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  return NBX_OK;
+}
+
+int nbx_status_bits(nbx_handle *h, uint32_t *bits) {
+  if (!h || !bits) return NBX_ERR_ARG;
+  NBX_CUDA(h, cudaMemcpyAsync(bits, h->base.status, 4, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaMemsetAsync(h->base.status, 0, 4, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  return NBX_OK;
+}
+
+const char *nbx_last_error(const nbx_handle *h) {
+  return h ? h->lastError.c_str() : "null handle";
+}
+
+} // extern "C"

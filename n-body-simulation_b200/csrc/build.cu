@@ -1,0 +1,548 @@
+// build.cu -- root square, Morton codes, Morton-order gather and the
+// quadtree build, for every instance of a handle in one launch per phase.
+//
+// The tree is the reference's Morton tree (src/cuda/TreeKernels.cuh:68-177,
+// driven as CudaQuadTree.cu:452-498): breadth-first node numbering, the 4
+// children of a node consecutive at `children`, `next` skip pointers, body
+// ranges [start, end), leaves of <= leafCapacity bodies (or at depth 32).
+//
+// The reference builds it level by level with grid-wide barriers.  Here
+// every level is built at once, straight from the sorted codes:
+//  * body i is the first body of the depth-d node containing it iff
+//    d > lcp(code[i-1], code[i]); that node splits iff it holds more than
+//    L bodies, i.e. code[i+L] shares its d-digit prefix, and d < 32.  So
+//    body i starts the splitting nodes of depths [lo_i, hi_i] with
+//    lo_i = lcp(i-1, i) + 1 and hi_i = min(lcp(i, i+L), 31);
+//  * the (segment, depth, first body) entries are bucketed by depth with a
+//    stable radix pass; a splitting node's rank among its level's
+//    splitting nodes is its position in its bucket, which fixes the BFS
+//    slot of its children (levelStart[d+1] + 4*rank), exactly the
+//    numbering of the serial loop;
+//  * centres are recomputed along the path from the root with the same
+//    float operations as splitNode (bit-identical), and `next` is the slot
+//    after the deepest ancestor that is not a last child;
+//  * mass / centre-of-mass (and second moments) go up the tree with
+//    arrival counters: the fourth child to finish sums its parent in the
+//    fixed order c0+c1+c2+c3 of sumNode, so the sums are deterministic.
+// A second pass lays the nodes out in depth-first preorder for the force
+// traversal (force.cu).
+#include "nbx_state.cuh"
+
+#include <float.h>
+
+namespace nbx {
+namespace {
+
+constexpr int kBlock = 256;
+
+int grid_for(uint32_t n) {
+  uint32_t b = (n + kBlock - 1) / kBlock;
+  if (b > 148u * 16u) b = 148u * 16u;
+  return b ? (int)b : 1;
+}
+
+__device__ __forceinline__ float key_to_float(uint32_t k) {
+  return u2f((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// Root square per instance (Quad::newContaining, QuadTree.cpp:30-51, and
+// rootSquare, CudaQuadTree.cu:25-30) and the Morton frame.  Resets the
+// bound accumulators for the next step.
+__global__ void k_root_frame(DevState S) {
+  const uint32_t sg = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sg >= S.nseg) return;
+  uint32_t *b = S.bounds + 4 * sg;
+  const float minX = b[0] == 0xffffffffu ? FLT_MAX : key_to_float(b[0]);
+  const float maxX = b[1] == 0u ? -FLT_MAX : key_to_float(b[1]);
+  const float minY = b[2] == 0xffffffffu ? FLT_MAX : key_to_float(b[2]);
+  const float maxY = b[3] == 0u ? -FLT_MAX : key_to_float(b[3]);
+  const float cx = __fmul_rn(__fadd_rn(minX, maxX), 0.5f);
+  const float cy = __fmul_rn(__fadd_rn(minY, maxY), 0.5f);
+  const float w = __fsub_rn(maxX, minX), h = __fsub_rn(maxY, minY);
+  const float size = (w < h) ? h : w;
+  SegDev &G = S.seg[sg];
+  G.cx = cx;
+  G.cy = cy;
+  G.size = size;
+  G.frame = sd_morton_frame(cx, cy, size);
+  b[0] = 0xffffffffu;
+  b[1] = 0u;
+  b[2] = 0xffffffffu;
+  b[3] = 0u;
+}
+
+// Morton code of every body; digit histograms of the 8 sort passes fused.
+__global__ void __launch_bounds__(kBlock)
+    k_morton(DevState S, uint64_t *__restrict__ keys, uint32_t *hist) {
+  __shared__ uint32_t sh[8][256];
+  for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) sh[i >> 8][i & 255] = 0;
+  __syncthreads();
+  const uint32_t n = S.n;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    const float4 p = S.pv[i];
+    const MortonFrame f = S.seg[S.segOf[i]].frame;
+    const uint64_t c = morton_code(p.x, p.y, f);
+    keys[i] = c;
+    S.codes[i] = c;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) atomicAdd(&sh[q][(c >> (8 * q)) & 255u], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) {
+    const uint32_t v = sh[i >> 8][i & 255];
+    if (v) atomicAdd(&hist[i], v);
+  }
+}
+
+// Sort key for the instance passes: segment of the element's original index.
+__global__ void k_seg_keys(DevState S, const uint32_t *__restrict__ vals,
+                           uint64_t *__restrict__ keys) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n;
+       i += gridDim.x * blockDim.x)
+    keys[i] = S.segOf[vals[i]];
+}
+
+// Permute the state into Morton order (the 7 gathers of
+// CudaQuadTree.cu:408-414, fused) and write the {x, y, m} traversal array.
+__global__ void __launch_bounds__(kBlock)
+    k_gather(DevState S, const uint32_t *__restrict__ perm) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t p = perm[i];
+    const float4 v = S.pv[p];
+    const float2 m = S.mr[p];
+    S.pv2[i] = v;
+    S.mr2[i] = m;
+    S.id2[i] = S.id[p];
+    S.xym[i] = make_float4(v.x, v.y, m.x, 0.0f);
+    S.perm[i] = p;
+    S.sortedCodes[i] = S.codes[p];
+  }
+}
+
+// ------------------------------------------------------------ tree build
+
+// Splitting nodes that start at body i: depths [lo, hi].
+__global__ void __launch_bounds__(kBlock) k_split_counts(DevState S) {
+  const uint64_t *c = S.sortedCodes;
+  const int L = S.leafCapacity;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n;
+       i += gridDim.x * blockDim.x) {
+    const SegDev &G = S.seg[S.segOf[i]];
+    const uint32_t s0 = G.start, s1 = G.start + G.count;
+    const int lo = (i == s0) ? 0 : lcp_digits(c[i - 1], c[i]) + 1;
+    int hi = -1;
+    if ((uint64_t)i + (uint32_t)L < s1) {
+      hi = lcp_digits(c[i], c[i + L]);
+      if (hi > kMaxDepth - 1) hi = kMaxDepth - 1;
+    }
+    const int cnt = hi >= lo ? hi - lo + 1 : 0;
+    S.splitCount[i] = (uint32_t)cnt;
+    S.splitLo[i] = (uint8_t)(lo > 255 ? 255 : lo);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_split_emit(DevState S, uint64_t *__restrict__ keys,
+                 uint32_t *__restrict__ vals) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t cnt = S.splitCount[i];
+    if (!cnt) continue;
+    const uint32_t base = S.splitStart[i];
+    const uint32_t lo = S.splitLo[i];
+    const uint64_t sg = S.segOf[i];
+    for (uint32_t k = 0; k < cnt; ++k) {
+      keys[base + k] = (sg << 6) | (lo + k);
+      vals[base + k] = i;
+    }
+  }
+}
+
+// Bucket boundaries of the depth-sorted entries.
+__global__ void __launch_bounds__(kBlock)
+    k_groups(DevState S, const uint64_t *__restrict__ keys) {
+  const uint32_t total = S.counters[3];
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += gridDim.x * blockDim.x) {
+    const uint64_t key = keys[k];
+    const uint32_t slot = (uint32_t)(key >> 6) * kLevelSlots + (uint32_t)(key & 63u);
+    if (k == 0 || keys[k - 1] != key) S.groupStart[slot] = k;
+    if (k + 1 == total || keys[k + 1] != key) S.groupEnd[slot] = k + 1;
+  }
+}
+
+// Level starts, node counts and node bases per instance; root nodes.
+__global__ void k_levels(DevState S) {
+  __shared__ uint32_t sRun;
+  if (threadIdx.x == 0) sRun = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < S.nseg; base += blockDim.x) {
+    const uint32_t sg = base + threadIdx.x;
+    uint32_t nodes = 0, levels = 0;
+    if (sg < S.nseg) {
+      SegDev &G = S.seg[sg];
+      uint32_t *ls = S.levelStart + sg * (kLevelSlots + 1);
+      const uint32_t *gs = S.groupStart + sg * kLevelSlots;
+      const uint32_t *ge = S.groupEnd + sg * kLevelSlots;
+      if (G.count > 0) {
+        ls[0] = 0;
+        ls[1] = 1;
+        uint32_t maxLevel = 0; // deepest level with nodes
+        for (int d = 1; d <= kMaxDepth; ++d) {
+          const uint32_t split = ge[d - 1] - gs[d - 1];
+          ls[d + 1] = ls[d] + 4u * split;
+          if (split) maxLevel = d;
+        }
+        nodes = ls[maxLevel + 1];
+        for (int d = maxLevel + 2; d <= kLevelSlots; ++d) ls[d] = nodes;
+        levels = maxLevel + 1;
+      } else {
+        for (int d = 0; d <= kLevelSlots; ++d) ls[d] = 0;
+      }
+      G.nodeCount = nodes;
+      G.levelCount = levels;
+    }
+    // block-wide exclusive scan of node counts -> node bases
+    __shared__ uint32_t sScan[1024];
+    sScan[threadIdx.x] = nodes;
+    __syncthreads();
+    for (uint32_t o = 1; o < blockDim.x; o <<= 1) {
+      const uint32_t v = threadIdx.x >= o ? sScan[threadIdx.x - o] : 0u;
+      __syncthreads();
+      sScan[threadIdx.x] += v;
+      __syncthreads();
+    }
+    const uint32_t excl = sRun + sScan[threadIdx.x] - nodes;
+    if (sg < S.nseg) {
+      SegDev &G = S.seg[sg];
+      G.nodeBase = excl;
+      if (excl + nodes <= S.nodeCapacity && nodes > 0) {
+        const uint32_t r = excl;
+        S.comX[r] = 0.0f;
+        S.comY[r] = 0.0f;
+        S.mass[r] = 0.0f;
+        S.centerX[r] = G.cx;
+        S.centerY[r] = G.cy;
+        S.size[r] = G.size;
+        S.children[r] = 0;
+        S.next[r] = 0;
+        S.start[r] = 0;
+        S.end[r] = (int32_t)G.count;
+        S.parent[r] = -1;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) sRun += sScan[blockDim.x - 1];
+    __syncthreads();
+  }
+  __syncthreads();
+  if (sRun > S.nodeCapacity) {
+    // all-or-nothing: no instance gets a tree, the step reports the error
+    for (uint32_t sg = threadIdx.x; sg < S.nseg; sg += blockDim.x)
+      S.seg[sg].nodeCount = 0;
+    if (threadIdx.x == 0) {
+      atomicOr(S.status, kStatusTreeCapacity);
+      S.counters[4] = 0;
+    }
+  } else if (threadIdx.x == 0) {
+    S.counters[4] = sRun;
+  }
+}
+
+// Index of the depth-t splitting node containing body i, by its rank.
+__device__ __forceinline__ uint32_t split_rank(const DevState &S,
+                                               const uint32_t *vals,
+                                               uint32_t sg, int t, uint32_t i) {
+  uint32_t lo = S.groupStart[sg * kLevelSlots + t];
+  uint32_t hi = S.groupEnd[sg * kLevelSlots + t];
+  const uint32_t g0 = lo;
+  // last position with vals[pos] <= i
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (vals[mid] <= i) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo > g0 ? lo - 1 - g0 : 0u; // the parent always exists
+}
+
+// firstWithDigit (TreeKernels.cuh:72-85) over global body indices.
+__device__ __forceinline__ uint32_t first_with_digit(const uint64_t *codes,
+                                                     uint32_t lo, uint32_t hi,
+                                                     int depth, int q) {
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (digit_at(codes[mid], depth) < q) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_split_nodes(DevState S, const uint64_t *__restrict__ keys,
+                  const uint32_t *__restrict__ vals) {
+  const uint32_t total = S.counters[3];
+  const uint64_t *codes = S.sortedCodes;
+  const uint32_t L = (uint32_t)S.leafCapacity;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += gridDim.x * blockDim.x) {
+    const uint64_t key = keys[k];
+    const uint32_t sg = (uint32_t)(key >> 6);
+    const int d = (int)(key & 63u);
+    const uint32_t i = vals[k];
+    if (sg >= S.nseg || d >= kMaxDepth) continue;
+    const SegDev &G = S.seg[sg];
+    if (G.nodeCount == 0) continue; // capacity overflow: instance skipped
+    const uint32_t nb = G.nodeBase;
+    const uint32_t s0 = G.start, s1 = G.start + G.count;
+    const uint32_t *ls = S.levelStart + sg * (kLevelSlots + 1);
+    const uint32_t r = k - S.groupStart[sg * kLevelSlots + d];
+    const uint64_t ci = codes[i];
+    uint32_t own = 0;
+    if (d > 0) own = ls[d] + 4u * split_rank(S, vals, sg, d - 1, i) +
+                     (uint32_t)digit_at(ci, d - 1);
+    const uint32_t childBase = ls[d + 1] + 4u * r;
+    if (childBase + 4 > G.nodeCount || own >= G.nodeCount) {
+      atomicOr(S.status, kStatusTreeCapacity);
+      continue;
+    }
+    // end of this node's body range
+    uint32_t end = s1;
+    if (d > 0) {
+      const uint64_t pre = ci >> (64 - 2 * d);
+      uint32_t lo = i + 1, hi = s1;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if ((codes[mid] >> (64 - 2 * d)) == pre) lo = mid + 1;
+        else hi = mid;
+      }
+      end = lo;
+    }
+    uint32_t bound[5];
+    bound[0] = i;
+    bound[4] = end;
+    for (int q = 1; q < 4; ++q)
+      bound[q] = first_with_digit(codes, bound[q - 1], end, d, q);
+    // centre and size along the path (splitNode's arithmetic)
+    float cx = G.cx, cy = G.cy, size = G.size;
+    for (int t = 0; t < d; ++t) {
+      size = __fmul_rn(size, 0.5f);
+      const int q = digit_at(ci, t);
+      cx = __fadd_rn(cx, __fmul_rn((float)(q & 1) - 0.5f, size));
+      cy = __fadd_rn(cy, __fmul_rn((float)(q >> 1) - 0.5f, size));
+    }
+    // own `next`: after the deepest ancestor-or-self that is not a last child
+    uint32_t ownNext = 0;
+    for (int t = d; t >= 1; --t) {
+      const int q = digit_at(ci, t - 1);
+      if (q < 3) {
+        const uint32_t idx =
+            (t == d) ? own
+                     : ls[t] + 4u * split_rank(S, vals, sg, t - 1, i) + (uint32_t)q;
+        ownNext = idx + 1;
+        break;
+      }
+    }
+    const float childSize = __fmul_rn(size, 0.5f);
+    S.children[nb + own] = (int32_t)childBase;
+    S.arrive[nb + own] = 0;
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t ch = nb + childBase + q;
+      S.comX[ch] = 0.0f;
+      S.comY[ch] = 0.0f;
+      S.mass[ch] = 0.0f;
+      S.centerX[ch] = __fadd_rn(cx, __fmul_rn((float)(q & 1) - 0.5f, childSize));
+      S.centerY[ch] = __fadd_rn(cy, __fmul_rn((float)(q >> 1) - 0.5f, childSize));
+      S.size[ch] = childSize;
+      S.next[ch] = (int32_t)(q < 3 ? childBase + q + 1 : ownNext);
+      S.start[ch] = (int32_t)(bound[q] - s0);
+      S.end[ch] = (int32_t)(bound[q + 1] - s0);
+      S.parent[ch] = (int32_t)own;
+      const bool splits = bound[q + 1] - bound[q] > L && d + 1 < kMaxDepth;
+      if (!splits) S.children[ch] = 0;
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t seg_of_node(const DevState &S, uint32_t g) {
+  uint32_t lo = 0, hi = S.nseg;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (S.seg[mid].nodeBase <= g) lo = mid;
+    else hi = mid;
+  }
+  // skip empty instances sharing the same base
+  while (lo + 1 < S.nseg && S.seg[lo].nodeCount == 0 && S.seg[lo + 1].nodeBase <= g)
+    ++lo;
+  return lo;
+}
+
+// Bottom-up pass: leaves sum their bodies (sumNode order), the last of
+// four children to finish sums their parent, then finishNode's divide.
+__global__ void __launch_bounds__(kBlock) k_upward(DevState S) {
+  const uint32_t total = S.counters[4];
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += gridDim.x * blockDim.x) {
+    if (S.children[g] != 0) continue;
+    const uint32_t sg = seg_of_node(S, g);
+    const SegDev &G = S.seg[sg];
+    const uint32_t nb = G.nodeBase, s0 = G.start;
+    const uint32_t b0 = s0 + (uint32_t)S.start[g], b1 = s0 + (uint32_t)S.end[g];
+    float px = 0.0f, py = 0.0f, mm = 0.0f;
+    for (uint32_t b = b0; b < b1; ++b) {
+      const float4 q = S.xym[b];
+      px = __fadd_rn(px, __fmul_rn(q.x, q.z));
+      py = __fadd_rn(py, __fmul_rn(q.y, q.z));
+      mm = __fadd_rn(mm, q.z);
+    }
+    const float div = fmaxf(mm, FLT_MIN);
+    const float X = __fdiv_rn(px, div), Y = __fdiv_rn(py, div);
+    float ixx = 0.0f, iyy = 0.0f, ixy = 0.0f;
+    for (uint32_t b = b0; b < b1; ++b) {
+      const float4 q = S.xym[b];
+      const float dx = q.x - X, dy = q.y - Y;
+      ixx += q.z * dx * dx;
+      iyy += q.z * dy * dy;
+      ixy += q.z * dx * dy;
+    }
+    S.sumX[g] = px;
+    S.sumY[g] = py;
+    S.mass[g] = mm;
+    S.comX[g] = X;
+    S.comY[g] = Y;
+    S.moments[g] = make_float4(ixx, iyy, ixy, 0.0f);
+    S.subtree[g] = 1;
+    // climb (at most kMaxDepth levels; parent indices are range-checked)
+    int32_t node = S.parent[g];
+    for (int guard = 0; node >= 0 && guard <= kMaxDepth; ++guard) {
+      if ((uint32_t)node >= G.nodeCount) {
+        atomicOr(S.status, kStatusTreeCapacity);
+        break;
+      }
+      const uint32_t pg = nb + (uint32_t)node;
+      __threadfence();
+      const uint32_t old = atomicAdd(&S.arrive[pg], 1u);
+      if (old != 3u) break;
+      __threadfence();
+      const uint32_t c = nb + (uint32_t)S.children[pg];
+      float sx = __ldcg(&S.sumX[c]), sy = __ldcg(&S.sumY[c]),
+            sm = __ldcg(&S.mass[c]);
+      uint32_t sub = 1 + __ldcg(&S.subtree[c]);
+      for (int q = 1; q < 4; ++q) {
+        sx = __fadd_rn(sx, __ldcg(&S.sumX[c + q]));
+        sy = __fadd_rn(sy, __ldcg(&S.sumY[c + q]));
+        sm = __fadd_rn(sm, __ldcg(&S.mass[c + q]));
+        sub += __ldcg(&S.subtree[c + q]);
+      }
+      const float dv = fmaxf(sm, FLT_MIN);
+      const float PX = __fdiv_rn(sx, dv), PY = __fdiv_rn(sy, dv);
+      float jxx = 0.0f, jyy = 0.0f, jxy = 0.0f;
+      for (int q = 0; q < 4; ++q) {
+        const float4 mo = __ldcg(&S.moments[c + q]);
+        const float cm = __ldcg(&S.mass[c + q]);
+        const float dx = __ldcg(&S.comX[c + q]) - PX;
+        const float dy = __ldcg(&S.comY[c + q]) - PY;
+        jxx += mo.x + cm * dx * dx;
+        jyy += mo.y + cm * dy * dy;
+        jxy += mo.z + cm * dx * dy;
+      }
+      __stcg(&S.sumX[pg], sx);
+      __stcg(&S.sumY[pg], sy);
+      __stcg(&S.mass[pg], sm);
+      __stcg(&S.comX[pg], PX);
+      __stcg(&S.comY[pg], PY);
+      __stcg(&S.moments[pg], make_float4(jxx, jyy, jxy, 0.0f));
+      __stcg(&S.subtree[pg], sub);
+      node = S.parent[pg];
+    }
+  }
+}
+
+// Preorder position of every node, and the traversal arrays.
+__global__ void __launch_bounds__(kBlock) k_preorder(DevState S) {
+  const uint32_t total = S.counters[4];
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += gridDim.x * blockDim.x) {
+    const uint32_t sg = seg_of_node(S, g);
+    const SegDev &G = S.seg[sg];
+    const uint32_t nb = G.nodeBase;
+    uint32_t pre = 0;
+    uint32_t cur = g - nb;
+    for (int guard = 0; cur != 0; ++guard) {
+      const uint32_t p = (uint32_t)S.parent[nb + cur];
+      if (p >= G.nodeCount || guard > kMaxDepth) {
+        atomicOr(S.status, kStatusTreeCapacity);
+        pre = 0;
+        break;
+      }
+      const uint32_t cb = (uint32_t)S.children[nb + p];
+      const uint32_t q = cur - cb;
+      pre += 1;
+      for (uint32_t t = 0; t < q; ++t) pre += S.subtree[nb + cb + t];
+      cur = p;
+    }
+    if (pre >= G.nodeCount) continue;
+    const uint32_t pg = nb + pre;
+    const float sz = S.size[g];
+    S.tA[pg] = make_float4(S.comX[g], S.comY[g], S.mass[g], __fmul_rn(sz, sz));
+    S.tB[pg] = make_int4((int)(pg + S.subtree[g]), (int)(G.start + S.start[g]),
+                         (int)(G.start + S.end[g]), S.children[g] == 0 ? 1 : 0);
+    const float4 mo = S.moments[g];
+    S.tM[pg] = make_float4(mo.x, mo.y, mo.z, sz);
+  }
+}
+
+} // namespace
+
+void launch_bounds(cudaStream_t s, const DevState &S);
+
+void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
+                  SortScratch &sort) {
+  const uint32_t n = S.n;
+  launch_bounds(s, S);
+  k_root_frame<<<(S.nseg + 127) / 128, 128, 0, s>>>(S);
+  cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * 8 * 256, s);
+  k_morton<<<grid_for(n), kBlock, 0, s>>>(S, sort.keys[0], sort.hist);
+  int buf = radix_sort_u64(s, sort, n, nullptr, 0, 64, true, true, S.status);
+  if (S.nseg > 1) {
+    // stable passes on the instance id keep instances in their ranges
+    k_seg_keys<<<grid_for(n), kBlock, 0, s>>>(S, sort.vals[buf], sort.keys[buf]);
+    if (buf == 1) {
+      cudaMemcpyAsync(sort.keys[0], sort.keys[1], sizeof(uint64_t) * n,
+                      cudaMemcpyDeviceToDevice, s);
+      cudaMemcpyAsync(sort.vals[0], sort.vals[1], sizeof(uint32_t) * n,
+                      cudaMemcpyDeviceToDevice, s);
+    }
+    const int segBits = S.nseg <= 256 ? 8 : 16;
+    buf = radix_sort_u64(s, sort, n, nullptr, 0, segBits, false, false, S.status);
+  }
+  k_gather<<<grid_for(n), kBlock, 0, s>>>(S, sort.vals[buf]);
+  // swap the double-buffered state: the host mirrors this swap
+  DevState T = S;
+  T.pv = S.pv2;
+  T.mr = S.mr2;
+  T.id = S.id2;
+  T.pv2 = S.pv;
+  T.mr2 = S.mr;
+  T.id2 = S.id;
+  S = T;
+  // tree
+  k_split_counts<<<grid_for(n), kBlock, 0, s>>>(S);
+  exclusive_scan_u32(s, S.splitCount, S.splitStart, n, nullptr, &S.counters[3],
+                     scan, S.status);
+  k_split_emit<<<grid_for(n), kBlock, 0, s>>>(S, sort.keys[0], sort.vals[0]);
+  const int depthBits = S.nseg <= 4 ? 8 : (S.nseg <= 1024 ? 16 : 24);
+  const int eb = radix_sort_u64(s, sort, 2 * n + 64, &S.counters[3], 0,
+                                depthBits, false, false, S.status);
+  cudaMemsetAsync(S.groupStart, 0, sizeof(uint32_t) * S.nseg * kLevelSlots, s);
+  cudaMemsetAsync(S.groupEnd, 0, sizeof(uint32_t) * S.nseg * kLevelSlots, s);
+  k_groups<<<grid_for(2 * n), kBlock, 0, s>>>(S, sort.keys[eb]);
+  k_levels<<<1, 1024, 0, s>>>(S);
+  k_split_nodes<<<grid_for(n / 4 + 64), kBlock, 0, s>>>(S, sort.keys[eb],
+                                                        sort.vals[eb]);
+  k_upward<<<grid_for(n), kBlock, 0, s>>>(S);
+  k_preorder<<<grid_for(n), kBlock, 0, s>>>(S);
+}
+
+} // namespace nbx

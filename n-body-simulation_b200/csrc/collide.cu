@@ -1,0 +1,562 @@
+// collide.cu -- integrate, collision broadphase and ordered resolution.
+//
+// Semantics follow the reference's CPU collide() (src/Collision.cpp:135-349):
+// the candidate set is every pair of boxes (pos -/+ radius) that overlaps
+// under before()/overlaps() (Collision.cpp:88-98), and pairs are resolved
+// one after another in pairLess order (Collision.cpp:333-348), each
+// resolve() seeing the previous ones' results.
+//
+// GPU design:
+//  * a hashed uniform grid (cell fixed per instance from the radii, as
+//    CudaCollision.cu:201-232 does) finds each small box's overlaps in its
+//    3x3 cell neighbourhood; boxes wider than ~a cell ("large", e.g. the
+//    central body) are tested against every box of their instance;
+//  * every body gets its partner list (CSR) sorted by the partners'
+//    before() order.  A body's chain of pairs in the global pairLess order
+//    is exactly that list: first the pairs where it is the later box
+//    (partners before it), then those where it is the earlier box;
+//  * resolution is a dataflow over "units" = bodies that are the later box
+//    of at least one pair, claimed in before() order.  A unit resolves its
+//    pairs in order; pair (L, E) waits until body E has completed the
+//    entries of its chain that precede L.  Units only ever wait on
+//    smaller units, so the smallest unfinished unit always progresses.
+//    The result equals the sequential loop bit for bit (the resolve
+//    arithmetic below is IEEE op for op, no contraction).
+#include "nbx_state.cuh"
+
+#include <float.h>
+
+namespace nbx {
+namespace {
+
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ uint32_t cell_hash(uint32_t seg, int cx, int cy,
+                                              uint32_t mask) {
+  uint32_t h = (uint32_t)cx * 0x9E3779B1u;
+  h ^= (uint32_t)cy * 0x85EBCA77u + (h << 6) + (h >> 2);
+  h ^= seg * 0xC2B2AE3Du;
+  h ^= h >> 15;
+  h *= 0x2C1B3C6Du;
+  h ^= h >> 13;
+  return h & mask;
+}
+
+// floor of the exact product v*inv (the reference takes the floor of the
+// double product, Collision.cpp:100-104).
+__device__ __forceinline__ int exact_floor_mul(float v, float inv) {
+  const float p = __fmul_rn(v, inv);
+  const float e = __fmaf_rn(v, inv, -p);
+  float f = floorf(p);
+  if (f == p && e < 0.0f) f -= 1.0f;
+  return (int)f;
+}
+
+// before(): Collision.cpp:88-90.
+__device__ __forceinline__ bool before_key(float aMinX, uint32_t a,
+                                           float bMinX, uint32_t b) {
+  return aMinX < bMinX || (aMinX == bMinX && a < b);
+}
+
+// overlaps(earlier, later): Collision.cpp:95-98.  box = {minX,maxX,minY,maxY}
+__device__ __forceinline__ bool boxes_overlap(const float4 &a, uint32_t ia,
+                                              const float4 &b, uint32_t ib) {
+  const bool aFirst = before_key(a.x, ia, b.x, ib);
+  const float4 &e = aFirst ? a : b;
+  const float4 &l = aFirst ? b : a;
+  return e.y >= l.x && l.z <= e.w && e.z <= l.w;
+}
+
+__device__ __forceinline__ bool is_small(const float4 &bx, float smallW) {
+  const float w = __fsub_rn(bx.y, bx.x), h = __fsub_rn(bx.w, bx.z);
+  return w <= smallW && h <= smallW;
+}
+
+// ---------------------------------------------------------------- kernels
+
+// Body::update (Body.h:20-23) for every body, then the collision box, the
+// grid cell and a slot in its bucket (or in its instance's large list).
+__global__ void __launch_bounds__(kBlock)
+    k_integrate_boxes(DevState S, int integrate, int collide) {
+  const uint32_t n = S.n;
+  const float dt = S.dt;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    float4 p = S.pv[i];
+    if (integrate) {
+      const float2 a = S.acc[i];
+      p.z = __fadd_rn(p.z, __fmul_rn(a.x, dt));
+      p.w = __fadd_rn(p.w, __fmul_rn(a.y, dt));
+      p.x = __fadd_rn(p.x, __fmul_rn(p.z, dt));
+      p.y = __fadd_rn(p.y, __fmul_rn(p.w, dt));
+      S.pv[i] = p;
+    }
+    if (!collide) continue;
+    const float r = S.mr[i].y;
+    const float4 bx = make_float4(__fsub_rn(p.x, r), __fadd_rn(p.x, r),
+                                  __fsub_rn(p.y, r), __fadd_rn(p.y, r));
+    S.box[i] = bx;
+    const uint32_t sg = S.segOf[i];
+    const SegDev &G = S.seg[sg];
+    bool small = is_small(bx, G.smallW);
+    int cx = 0, cy = 0;
+    if (small) {
+      const float fx = __fmul_rn(bx.x, G.invCell);
+      const float fy = __fmul_rn(bx.z, G.invCell);
+      // far from the origin the float cell index loses integer precision:
+      // such boxes are treated as large (compared against everything).
+      if (!(fabsf(fx) < 8388608.0f && fabsf(fy) < 8388608.0f)) {
+        small = false;
+      } else {
+        cx = exact_floor_mul(bx.x, G.invCell);
+        cy = exact_floor_mul(bx.z, G.invCell);
+      }
+    }
+    if (small) {
+      const uint32_t h = cell_hash(sg, cx, cy, S.nBuckets - 1);
+      S.slot[i] = atomicAdd(&S.bucketCount[h], 1u);
+      S.cellXY[i] = make_int2(cx, cy);
+    } else {
+      S.slot[i] = atomicAdd(&S.largeCount[sg], 1u) | 0x80000000u;
+      S.cellXY[i] = make_int2(0x7fffffff, 0x7fffffff);
+      S.deg[i] = 0;       // accumulated by the partners' atomics
+      S.fillLarge[i] = 0; // fill cursor of this large body's list
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_fill_grid(DevState S) {
+  const uint32_t n = S.n;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t s = S.slot[i];
+    const uint32_t sg = S.segOf[i];
+    if (s & 0x80000000u) {
+      S.largeList[S.largeStartA[sg] + (s & 0x7fffffffu)] = i;
+    } else {
+      const int2 c = S.cellXY[i];
+      const uint32_t h = cell_hash(sg, c.x, c.y, S.nBuckets - 1);
+      S.grid[S.bucketStart[h] + s] = i;
+    }
+  }
+}
+
+// Partner discovery.  kFill = false counts, kFill = true writes the lists
+// (small bodies sort their own list in place).
+template <bool kFill>
+__global__ void __launch_bounds__(kBlock) k_partners(DevState S) {
+  const uint32_t n = S.n;
+  const uint32_t mask = S.nBuckets - 1;
+  const uint32_t cap = S.pairCapacity;
+  const bool overflow = kFill && S.counters[0] > cap;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t sg = S.segOf[i];
+    const float4 bi = S.box[i];
+    const uint32_t lStart = S.largeStartA[sg];
+    const uint32_t lCount = S.largeCount[sg];
+    const bool iLarge = (S.slot[i] & 0x80000000u) != 0;
+    uint32_t cnt = 0;
+    uint32_t base = kFill ? S.pstart[i] : 0u;
+    if (!iLarge) {
+      const int2 c = S.cellXY[i];
+      for (int dy = -1; dy <= 1; ++dy) {
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int ncx = c.x + dx, ncy = c.y + dy;
+          const uint32_t h = cell_hash(sg, ncx, ncy, mask);
+          const uint32_t e0 = S.bucketStart[h], e1 = S.bucketStart[h + 1];
+          for (uint32_t e = e0; e < e1; ++e) {
+            const uint32_t j = S.grid[e];
+            if (j == i) continue;
+            const int2 cj = S.cellXY[j];
+            if (cj.x != ncx || cj.y != ncy || S.segOf[j] != sg) continue;
+            const float4 bj = S.box[j];
+            if (boxes_overlap(bi, i, bj, j)) {
+              if (kFill && !overflow) S.plist[base + cnt] = j;
+              ++cnt;
+            }
+          }
+        }
+      }
+      for (uint32_t k = 0; k < lCount; ++k) {
+        const uint32_t j = S.largeList[lStart + k];
+        const float4 bj = S.box[j];
+        if (boxes_overlap(bi, i, bj, j)) {
+          if (kFill) {
+            if (!overflow) {
+              S.plist[base + cnt] = j;
+              const uint32_t slotJ = atomicAdd(&S.fillLarge[j], 1u);
+              S.plist[S.pstart[j] + slotJ] = i;
+            }
+          } else {
+            atomicAdd(&S.deg[j], 1u);
+          }
+          ++cnt;
+        }
+      }
+      if (!kFill) {
+        S.deg[i] = cnt;
+      } else if (overflow) {
+        S.nLater[i] = 0;
+        S.unitFlag[i] = 0;
+        if (i == 0) atomicOr(S.status, kStatusPairCapacity);
+      } else {
+        // insertion sort of the own list by the partners' before() order
+        uint32_t nl = 0;
+        for (uint32_t a = 1; a < cnt; ++a) {
+          const uint32_t v = S.plist[base + a];
+          const float vk = S.box[v].x;
+          uint32_t b = a;
+          while (b > 0) {
+            const uint32_t u = S.plist[base + b - 1];
+            if (!before_key(vk, v, S.box[u].x, u)) break;
+            S.plist[base + b] = u;
+            --b;
+          }
+          S.plist[base + b] = v;
+        }
+        for (uint32_t a = 0; a < cnt; ++a) {
+          const uint32_t u = S.plist[base + a];
+          if (before_key(S.box[u].x, u, bi.x, i)) ++nl;
+        }
+        S.nLater[i] = nl;
+        S.unitFlag[i] = nl > 0 ? 1u : 0u;
+      }
+    } else {
+      // large vs large (both directions are visited; each side records
+      // its own half)
+      for (uint32_t k = 0; k < lCount; ++k) {
+        const uint32_t j = S.largeList[lStart + k];
+        if (j == i) continue;
+        const float4 bj = S.box[j];
+        if (boxes_overlap(bi, i, bj, j)) {
+          if (kFill) {
+            if (!overflow) {
+              const uint32_t slotI = atomicAdd(&S.fillLarge[i], 1u);
+              S.plist[S.pstart[i] + slotI] = j;
+            }
+          }
+          ++cnt;
+        }
+      }
+      if (!kFill) atomicAdd(&S.deg[i], cnt);
+    }
+  }
+}
+
+// Sorts each large body's partner list (filled by others through atomics)
+// by before() order: one warp per large body, rank by counting.
+__global__ void __launch_bounds__(kBlock) k_sort_large(DevState S) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warpId = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nWarps = (gridDim.x * blockDim.x) >> 5;
+  const bool overflow = S.counters[0] > S.pairCapacity;
+  // large bodies of all instances, back to back in the large list
+  const uint32_t totalLarge =
+      S.largeStartA[S.nseg - 1] + S.largeCount[S.nseg - 1];
+  for (uint32_t w = warpId; w < totalLarge; w += nWarps) {
+    const uint32_t g = S.largeList[w];
+    const uint32_t d = S.deg[g];
+    const uint32_t base = S.pstart[g];
+    const float gk = S.box[g].x;
+    if (!overflow && d > 0) {
+      // rank of each element, written to the scratch copy of the lists
+      for (uint32_t a = lane; a < d; a += 32) {
+        const uint32_t v = S.plist[base + a];
+        const float vk = S.box[v].x;
+        uint32_t rank = 0;
+        for (uint32_t b = 0; b < d; ++b) {
+          const uint32_t u = S.plist[base + b];
+          rank += before_key(S.box[u].x, u, vk, v) ? 1u : 0u;
+        }
+        S.plistTmp[base + rank] = v;
+      }
+      __syncwarp();
+      uint32_t nl = 0;
+      for (uint32_t a = lane; a < d; a += 32) {
+        const uint32_t u = S.plistTmp[base + a];
+        S.plist[base + a] = u;
+        nl += before_key(S.box[u].x, u, gk, g) ? 1u : 0u;
+      }
+      for (int o = 16; o > 0; o >>= 1) nl += __shfl_xor_sync(0xffffffffu, nl, o);
+      if (lane == 0) {
+        S.nLater[g] = nl;
+        S.unitFlag[g] = nl > 0 ? 1u : 0u;
+      }
+    } else if (lane == 0) {
+      S.nLater[g] = 0;
+      S.unitFlag[g] = 0;
+    }
+  }
+}
+
+// Units (bodies that are the later box of >= 1 pair), in index order, keyed
+// by their minX for the before()-order sort.
+__global__ void __launch_bounds__(kBlock) k_units(DevState S, uint64_t *keys,
+                                                  uint32_t *vals) {
+  const uint32_t n = S.n;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    if (S.unitFlag[i]) {
+      const uint32_t p = S.unitPos[i];
+      keys[p] = float_order_key(S.box[i].x);
+      vals[p] = i;
+    }
+  }
+}
+
+// resolve(bodies, i = later, j = earlier): Collision.cpp:16-84, IEEE op
+// for op.  s = {x, y, vx, vy}.
+__device__ void resolve_pair(float4 &s1, float m1, float r1, float4 &s2,
+                             float m2, float r2) {
+  float dx = __fsub_rn(s2.x, s1.x), dy = __fsub_rn(s2.y, s1.y);
+  const float r = __fadd_rn(r1, r2);
+  const float dd = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+  if (dd > __fmul_rn(r, r)) return;
+  const float v1x = s1.z, v1y = s1.w, v2x = s2.z, v2y = s2.w;
+  const float vx = __fsub_rn(v2x, v1x), vy = __fsub_rn(v2y, v1y);
+  float dDotV = __fadd_rn(__fmul_rn(dx, vx), __fmul_rn(dy, vy));
+  const float msum = __fadd_rn(m1, m2);
+  const float w1 = __fdiv_rn(m2, msum);
+  const float w2 = __fdiv_rn(m1, msum);
+  const bool dNonZero = !(dx == 0.0f && dy == 0.0f);
+  if (dDotV >= 0.0f && dNonZero) {
+    const float s = __fsub_rn(__fdiv_rn(r, __fsqrt_rn(dd)), 1.0f);
+    const float tx = __fmul_rn(dx, s), ty = __fmul_rn(dy, s);
+    s1.x = __fsub_rn(s1.x, __fmul_rn(w1, tx));
+    s1.y = __fsub_rn(s1.y, __fmul_rn(w1, ty));
+    s2.x = __fadd_rn(s2.x, __fmul_rn(w2, tx));
+    s2.y = __fadd_rn(s2.y, __fmul_rn(w2, ty));
+    return;
+  }
+  const float vSq = __fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy));
+  if (vSq < 1e-12f) {
+    float dirX = 1.0f, dirY = 0.0f;
+    if (dNonZero) {
+      const float inv = __fdiv_rn(1.0f, __fsqrt_rn(dd));
+      dirX = __fmul_rn(dx, inv);
+      dirY = __fmul_rn(dy, inv);
+    }
+    const float tx = __fmul_rn(dirX, r), ty = __fmul_rn(dirY, r);
+    s1.x = __fsub_rn(s1.x, __fmul_rn(w1, tx));
+    s1.y = __fsub_rn(s1.y, __fmul_rn(w1, ty));
+    s2.x = __fadd_rn(s2.x, __fmul_rn(w2, tx));
+    s2.y = __fadd_rn(s2.y, __fmul_rn(w2, ty));
+    return;
+  }
+  const float rSq = __fmul_rn(r, r);
+  const float disc = fmaxf(
+      __fsub_rn(__fmul_rn(dDotV, dDotV), __fmul_rn(vSq, __fsub_rn(dd, rSq))),
+      0.0f);
+  const float t = __fdiv_rn(__fadd_rn(dDotV, __fsqrt_rn(disc)), vSq);
+  s1.x = __fsub_rn(s1.x, __fmul_rn(v1x, t));
+  s1.y = __fsub_rn(s1.y, __fmul_rn(v1y, t));
+  s2.x = __fsub_rn(s2.x, __fmul_rn(v2x, t));
+  s2.y = __fsub_rn(s2.y, __fmul_rn(v2y, t));
+  dx = __fsub_rn(s2.x, s1.x);
+  dy = __fsub_rn(s2.y, s1.y);
+  dDotV = __fadd_rn(__fmul_rn(dx, vx), __fmul_rn(dy, vy));
+  const float dSq2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+  const float s = __fdiv_rn(__fmul_rn(1.5f, dDotV), dSq2);
+  const float tx = __fmul_rn(dx, s), ty = __fmul_rn(dy, s);
+  const float n1x = __fadd_rn(v1x, __fmul_rn(tx, w1));
+  const float n1y = __fadd_rn(v1y, __fmul_rn(ty, w1));
+  const float n2x = __fsub_rn(v2x, __fmul_rn(tx, w2));
+  const float n2y = __fsub_rn(v2y, __fmul_rn(ty, w2));
+  s1.z = n1x;
+  s1.w = n1y;
+  s2.z = n2x;
+  s2.w = n2y;
+  s1.x = __fadd_rn(s1.x, __fmul_rn(n1x, t));
+  s1.y = __fadd_rn(s1.y, __fmul_rn(n1y, t));
+  s2.x = __fadd_rn(s2.x, __fmul_rn(n2x, t));
+  s2.y = __fadd_rn(s2.y, __fmul_rn(n2y, t));
+}
+
+// Position of body `who` in body e's sorted partner list.
+__device__ __forceinline__ uint32_t chain_position(const DevState &S,
+                                                   uint32_t e, uint32_t who,
+                                                   float whoKey) {
+  uint32_t lo = 0, hi = S.deg[e];
+  const uint32_t base = S.pstart[e];
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    const uint32_t u = S.plist[base + mid];
+    if (before_key(S.box[u].x, u, whoKey, who)) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_resolve(DevState S, const uint32_t *__restrict__ units) {
+  const uint32_t numUnits = S.counters[1];
+  const int lane = threadIdx.x & 31;
+  if (S.counters[0] > S.pairCapacity) return;
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&S.counters[2], 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= numUnits) break;
+    const uint32_t u = base + lane;
+    if (u < numUnits) {
+      const uint32_t L = units[u];
+      S.unitOrder[u] = L; // kept for introspection of the pair order
+      const uint32_t nl = S.nLater[L];
+      const uint32_t pl = S.pstart[L];
+      const float lKey = S.box[L].x;
+      const float2 mrL = S.mr[L];
+      float4 sL = S.pv[L];
+      bool ok = true;
+      for (uint32_t k = 0; k < nl && ok; ++k) {
+        const uint32_t E = S.plist[pl + k];
+        const uint32_t m = chain_position(S, E, L, lKey);
+        uint32_t spins = 0;
+        while (ld_acquire_u32(&S.prog[E]) != m) {
+          if (++spins > kSpinLimit) {
+            atomicOr(S.status, kStatusSpinLimit);
+            ok = false;
+            break;
+          }
+          __nanosleep(128);
+        }
+        if (!ok) break;
+        const float2 mrE = S.mr[E];
+        float4 sE = __ldcg(&S.pv[E]);
+        resolve_pair(sL, mrL.x, mrL.y, sE, mrE.x, mrE.y);
+        __stcg(&S.pv[E], sE);
+        __threadfence();
+        st_release_u32(&S.prog[E], m + 1);
+      }
+      __stcg(&S.pv[L], sL);
+      __threadfence();
+      st_release_u32(&S.prog[L], nl);
+    }
+  }
+}
+
+// Bounding boxes per instance: each block takes a contiguous chunk;
+// per-thread min/max keys, block-reduced when the whole block is in one
+// instance, flushed with atomics otherwise.
+__global__ void __launch_bounds__(kBlock) k_bounds(DevState S) {
+  const uint32_t n = S.n;
+  const uint32_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const uint32_t c0 = blockIdx.x * chunk;
+  const uint32_t c1 = min(n, c0 + chunk);
+  __shared__ uint32_t sb[4];
+  __shared__ uint32_t sSeg;
+  if (threadIdx.x == 0) {
+    sb[0] = 0xffffffffu;
+    sb[1] = 0u;
+    sb[2] = 0xffffffffu;
+    sb[3] = 0u;
+    sSeg = c0 < c1 ? S.segOf[c1 - 1] : 0xffffffffu;
+  }
+  __syncthreads();
+  uint32_t curSeg = 0xffffffffu;
+  uint32_t k0 = 0xffffffffu, k1 = 0u, k2 = 0xffffffffu, k3 = 0u;
+  bool any = false;
+  for (uint32_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+    const uint32_t sg = S.segOf[i];
+    if (sg != curSeg) {
+      if (any) {
+        uint32_t *b = S.bounds + 4 * curSeg;
+        atomicMin(b + 0, k0);
+        atomicMax(b + 1, k1);
+        atomicMin(b + 2, k2);
+        atomicMax(b + 3, k3);
+      }
+      curSeg = sg;
+      k0 = 0xffffffffu;
+      k1 = 0u;
+      k2 = 0xffffffffu;
+      k3 = 0u;
+      any = false;
+    }
+    const float4 p = S.pv[i];
+    if (!(fabsf(p.x) <= FLT_MAX && fabsf(p.y) <= FLT_MAX)) {
+      if (p.x != p.x || p.y != p.y || fabsf(p.x) > FLT_MAX || fabsf(p.y) > FLT_MAX)
+        atomicOr(S.status, kStatusNonFinite);
+      if (p.x != p.x || p.y != p.y) continue; // NaN never wins a min/max
+    }
+    const uint32_t kx = float_order_key(p.x), ky = float_order_key(p.y);
+    k0 = min(k0, kx);
+    k1 = max(k1, kx);
+    k2 = min(k2, ky);
+    k3 = max(k3, ky);
+    any = true;
+  }
+  if (any) {
+    if (curSeg == sSeg) {
+      atomicMin(&sb[0], k0);
+      atomicMax(&sb[1], k1);
+      atomicMin(&sb[2], k2);
+      atomicMax(&sb[3], k3);
+    } else {
+      uint32_t *b = S.bounds + 4 * curSeg;
+      atomicMin(b + 0, k0);
+      atomicMax(b + 1, k1);
+      atomicMin(b + 2, k2);
+      atomicMax(b + 3, k3);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && sSeg != 0xffffffffu && sb[1] != 0u) {
+    uint32_t *b = S.bounds + 4 * sSeg;
+    atomicMin(b + 0, sb[0]);
+    atomicMax(b + 1, sb[1]);
+    atomicMin(b + 2, sb[2]);
+    atomicMax(b + 3, sb[3]);
+  }
+}
+
+int grid_for(uint32_t n) {
+  uint32_t b = (n + kBlock - 1) / kBlock;
+  if (b > 148u * 16u) b = 148u * 16u;
+  return b ? (int)b : 1;
+}
+
+} // namespace
+
+// Host-side sequencing of the collision phase (no host synchronisation).
+void launch_integrate(cudaStream_t s, const DevState &S, bool integrate,
+                      bool collide) {
+  k_integrate_boxes<<<grid_for(S.n), kBlock, 0, s>>>(S, integrate ? 1 : 0,
+                                                     collide ? 1 : 0);
+}
+
+void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
+                    SortScratch &sort) {
+  const uint32_t n = S.n;
+  // grid buckets and large lists
+  exclusive_scan_u32(s, S.bucketCount, S.bucketStart, S.nBuckets + 1, nullptr,
+                     nullptr, scan, S.status);
+  exclusive_scan_u32(s, S.largeCount, S.largeStartA, S.nseg, nullptr, nullptr,
+                     scan, S.status);
+  k_fill_grid<<<grid_for(n), kBlock, 0, s>>>(S);
+  // partners: count, scan, fill + sort
+  k_partners<false><<<grid_for(n), kBlock, 0, s>>>(S);
+  exclusive_scan_u32(s, S.deg, S.pstart, n, nullptr, &S.counters[0], scan,
+                     S.status);
+  k_partners<true><<<grid_for(n), kBlock, 0, s>>>(S);
+  k_sort_large<<<64, kBlock, 0, s>>>(S);
+  // units in before() order
+  exclusive_scan_u32(s, S.unitFlag, S.unitPos, n, nullptr, &S.counters[1],
+                     scan, S.status);
+  k_units<<<grid_for(n), kBlock, 0, s>>>(S, sort.keys[0], sort.vals[0]);
+  const int buf = radix_sort_u64(s, sort, n, &S.counters[1], 0, 32, false,
+                                 false, S.status);
+  // ordered resolution
+  cudaMemsetAsync(S.prog, 0, sizeof(uint32_t) * n, s);
+  cudaMemsetAsync(&S.counters[2], 0, sizeof(uint32_t), s);
+  k_resolve<<<148 * 8, kBlock, 0, s>>>(S, sort.vals[buf]);
+}
+
+void launch_bounds(cudaStream_t s, const DevState &S) {
+  uint32_t blocks = (S.n + 4095) / 4096;
+  if (blocks > 148u * 8u) blocks = 148u * 8u;
+  if (blocks < 1) blocks = 1;
+  k_bounds<<<blocks, kBlock, 0, s>>>(S);
+}
+
+} // namespace nbx

@@ -1,0 +1,175 @@
+// force.cu -- warp-cooperative stackless Barnes-Hut traversal.
+//
+// Each lane walks the tree for one body exactly as accelerationAt does
+// (src/cuda/TreeKernels.cuh:197-245; QuadTree::acceleration,
+// src/QuadTree.cpp:264-389): accept a node when size^2 < d^2*theta^2 and
+// add m*d*fastInvSqrt(d^2)/(d^2+eps^2) (clamped to FLT_MAX), otherwise sum
+// a leaf's bodies one by one, otherwise descend.  Per-lane acceptance is
+// kept, so each body opens exactly the nodes the reference opens and sums
+// them in the same order.
+//
+// The warp cooperates through the depth-first preorder layout (build.cu):
+// along every lane's walk the preorder position only increases (descend =
+// +1, skip = +subtree size), so the warp always serves the smallest
+// position any lane is waiting at.  The lanes at that node evaluate it
+// together from one shared-memory copy; tiles of the next 32 nodes are
+// staged into shared memory with one coalesced load, and a leaf's bodies
+// likewise, so the walk does not pay a dependent global load per node.
+//
+// kExact = true evaluates every float operation as the reference writes
+// it (no FMA contraction, IEEE reciprocal): the result is bit-identical to
+// the host-compiled reference traversal on the same tree.  kExact = false
+// lets the compiler contract and uses the hardware reciprocal
+// approximation (relative difference ~1e-7 per term).
+#include "nbx_state.cuh"
+
+#include <float.h>
+
+namespace nbx {
+namespace {
+
+constexpr int kForceBlock = 256;
+constexpr int kWarps = kForceBlock / 32;
+constexpr uint32_t kDone = 0xffffffffu;
+
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+template <bool kExact>
+__device__ __forceinline__ float inv_sqrt_law(float x) {
+  if (kExact) {
+    const float xhalf = __fmul_rn(0.5f, x);
+    const float y = u2f(0x5f3759dfu - (f2u(x) >> 1));
+    return __fmul_rn(y, __fsub_rn(1.5f, __fmul_rn(__fmul_rn(xhalf, y), y)));
+  } else {
+    return fast_inv_sqrt(x);
+  }
+}
+
+// One interaction of the tree force law; accumulates into (ax, ay).
+template <bool kExact>
+__device__ __forceinline__ void add_term(float dx, float dy, float dSq,
+                                         float m, float eSq, float &ax,
+                                         float &ay) {
+  if (kExact) {
+    const float f = fminf(__fmul_rn(__fmul_rn(m, inv_sqrt_law<true>(dSq)),
+                                    __frcp_rn(__fadd_rn(dSq, eSq))),
+                          FLT_MAX);
+    ax = __fadd_rn(ax, __fmul_rn(dx, f));
+    ay = __fadd_rn(ay, __fmul_rn(dy, f));
+  } else {
+    const float f =
+        fminf(m * inv_sqrt_law<false>(dSq) * rcp_approx(dSq + eSq), FLT_MAX);
+    ax = fmaf(dx, f, ax);
+    ay = fmaf(dy, f, ay);
+  }
+}
+
+template <bool kExact>
+__device__ __forceinline__ float sq_dist(float dx, float dy) {
+  if (kExact) return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+  return fmaf(dx, dx, dy * dy);
+}
+
+template <bool kExact>
+__global__ void __launch_bounds__(kForceBlock)
+    k_forces(DevState S, float tSq, float eSq) {
+  __shared__ float4 sA[kWarps][32];
+  __shared__ int4 sB[kWarps][32];
+  __shared__ float4 sBody[kWarps][32];
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  const uint32_t totalNodes = S.counters[4];
+  const uint32_t warpsTotal = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t wb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+       wb < S.n; wb += warpsTotal * 32) {
+    const uint32_t i = wb + lane;
+    const bool valid = i < S.n;
+    float x = 0.0f, y = 0.0f;
+    uint32_t cur = kDone, endNode = 0;
+    if (valid) {
+      const float4 b = S.xym[i];
+      x = b.x;
+      y = b.y;
+      const SegDev &G = S.seg[S.segOf[i]];
+      if (G.nodeCount > 0) {
+        cur = G.nodeBase;
+        endNode = G.nodeBase + G.nodeCount;
+      }
+    }
+    float ax = 0.0f, ay = 0.0f;
+    uint32_t tileBase = kDone;
+    for (;;) {
+      const uint32_t k = __reduce_min_sync(0xffffffffu, cur);
+      if (k == kDone) break;
+      if (tileBase == kDone || k < tileBase || k >= tileBase + 32) {
+        tileBase = k;
+        const uint32_t g = k + lane;
+        if (g < totalNodes) {
+          sA[w][lane] = S.tA[g];
+          sB[w][lane] = S.tB[g];
+        }
+        __syncwarp();
+      }
+      const float4 A = sA[w][k - tileBase];
+      const int4 B = sB[w][k - tileBase];
+      bool openLeaf = false;
+      if (cur == k) {
+        const float dx = kExact ? __fsub_rn(A.x, x) : A.x - x;
+        const float dy = kExact ? __fsub_rn(A.y, y) : A.y - y;
+        const float dSq = sq_dist<kExact>(dx, dy);
+        const float far = kExact ? __fmul_rn(dSq, tSq) : dSq * tSq;
+        if (A.w < far) {
+          if (A.z > 0.0f) add_term<kExact>(dx, dy, dSq, A.z, eSq, ax, ay);
+          cur = (uint32_t)B.x > k ? (uint32_t)B.x : kDone;
+        } else if (B.w) {
+          openLeaf = true;
+        } else {
+          cur = k + 1;
+        }
+      }
+      const uint32_t leafLanes = __ballot_sync(0xffffffffu, openLeaf);
+      if (leafLanes) {
+        const uint32_t b0 = (uint32_t)B.y, b1 = (uint32_t)B.z;
+        const uint32_t bEnd = b1 <= S.n ? b1 : S.n; // defensive bound
+        for (uint32_t base = b0; base < bEnd; base += 32) {
+          const uint32_t cnt = min(32u, bEnd - base);
+          __syncwarp();
+          if ((uint32_t)lane < cnt) sBody[w][lane] = S.xym[base + lane];
+          __syncwarp();
+          if (openLeaf) {
+            for (uint32_t j = 0; j < cnt; ++j) {
+              const float4 q = sBody[w][j];
+              const float ex = kExact ? __fsub_rn(q.x, x) : q.x - x;
+              const float ey = kExact ? __fsub_rn(q.y, y) : q.y - y;
+              add_term<kExact>(ex, ey, sq_dist<kExact>(ex, ey), q.z, eSq, ax,
+                               ay);
+            }
+          }
+        }
+        if (openLeaf) cur = (uint32_t)B.x > k ? (uint32_t)B.x : kDone;
+      }
+      if (cur != kDone && cur >= endNode) cur = kDone;
+    }
+    if (valid) S.acc[i] = make_float2(ax, ay);
+  }
+}
+
+} // namespace
+
+void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks) {
+  if (blocks <= 0) {
+    uint32_t warps = (S.n + 31) / 32;
+    uint32_t b = (warps + kWarps - 1) / kWarps;
+    blocks = (int)(b ? b : 1);
+  }
+  if (exact)
+    k_forces<true><<<blocks, kForceBlock, 0, s>>>(S, S.tSq, S.eSq);
+  else
+    k_forces<false><<<blocks, kForceBlock, 0, s>>>(S, S.tSq, S.eSq);
+}
+
+} // namespace nbx

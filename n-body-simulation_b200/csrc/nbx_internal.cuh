@@ -1,0 +1,113 @@
+// nbx_internal.cuh -- device-side building blocks shared by the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "nbx_math.h"
+
+namespace nbx {
+
+// Error bits collected in the device status word (Handle::status).
+enum StatusBits : uint32_t {
+  kStatusOk = 0,
+  kStatusSpinLimit = 1u << 0,    // a bounded wait gave up
+  kStatusTreeCapacity = 1u << 1, // node capacity would have been exceeded
+  kStatusPairCapacity = 1u << 2, // collision partner capacity exceeded
+  kStatusNonFinite = 1u << 3,    // a body position became NaN/inf
+  kStatusLargeCapacity = 1u << 4,
+  kStatusBadSegment = 1u << 5,
+};
+
+// Iteration cap of every spin-wait in this library (each iteration sleeps
+// ~64-256 ns, so this bounds a wait at well under a few seconds).
+constexpr uint32_t kSpinLimit = 1u << 23;
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(uint32_t *p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t *p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(uint64_t *p, uint64_t v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u32(uint32_t *p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Grid-stride helpers sized from a device-side count.
+__device__ __forceinline__ uint32_t load_count(const uint32_t *d_n, uint32_t n) {
+  return d_n ? *d_n : n;
+}
+
+// ---------------------------------------------------------------------
+// Device-wide primitives (scan_sort.cu).  All take a stream and never
+// synchronise with the host, so they can be captured in a CUDA graph.
+struct ScanScratch {
+  uint64_t *status = nullptr; // one word per tile
+  uint32_t *tileCounter = nullptr;
+  uint32_t maxTiles = 0;
+};
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+// out[i] = sum(in[0..i)) for i < n; if total != nullptr it receives the sum.
+// n is *d_n when d_n != nullptr (n_max bounds the launch).
+void exclusive_scan_u32(cudaStream_t s, const uint32_t *in, uint32_t *out,
+                        uint32_t n_max, const uint32_t *d_n, uint32_t *total,
+                        ScanScratch &sc, uint32_t *err);
+size_t scan_scratch_tiles(uint32_t n_max);
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 12;
+constexpr int kSortTile = kSortThreads * kSortItems; // 3072
+constexpr int kSortWarps = kSortThreads / 32;
+
+struct SortScratch {
+  uint64_t *keys[2] = {nullptr, nullptr};
+  uint32_t *vals[2] = {nullptr, nullptr};
+  uint32_t *hist = nullptr;        // [8 passes][256] digit counts
+  uint32_t *status = nullptr;      // [maxTiles][256] look-back words
+  uint32_t *tileCounter = nullptr; // [8]
+  uint32_t maxTiles = 0;
+  uint32_t capacity = 0;
+};
+
+size_t sort_tiles(uint32_t n_max);
+
+// Stable LSD radix sort of (keys[0], vals[0]) on key bits [bit_lo, bit_hi)
+// (multiples of 8).  If `have_hist` the caller already filled
+// scratch.hist for those passes (e.g. fused into the key-producing
+// kernel) and zeroed nothing else.  vals_identity: vals[0] is not read,
+// value = original index.  Returns the buffer index (0/1) holding the
+// result.
+int radix_sort_u64(cudaStream_t s, SortScratch &sc, uint32_t n_max,
+                   const uint32_t *d_n, int bit_lo, int bit_hi,
+                   bool vals_identity, bool have_hist, uint32_t *err);
+
+// Digit histograms of keys for passes [bit_lo, bit_hi) (zeroes them first).
+void radix_histogram(cudaStream_t s, SortScratch &sc, const uint64_t *keys,
+                     uint32_t n_max, const uint32_t *d_n, int bit_lo,
+                     int bit_hi);
+
+} // namespace nbx

@@ -1,0 +1,105 @@
+// nbx_state.cuh -- device state of one simulation handle (one or many
+// independent instances, "segments", laid out back to back).
+#pragma once
+#include "nbx_internal.cuh"
+
+namespace nbx {
+
+// Per-segment record in device memory.
+struct SegDev {
+  uint32_t start, count;       // body range [start, start+count)
+  float cell, invCell, smallW; // collision grid cell; boxes wider than
+                               // smallW go to the large list
+  uint32_t pad0;
+  // written every step
+  float cx, cy, size; // root square (Quad::newContaining)
+  uint32_t pad1;
+  MortonFrame frame;  // quantisation constants (binary64 bit patterns)
+  uint32_t nodeBase;  // first node of this segment's tree
+  uint32_t nodeCount; // nodes in this segment's tree
+  uint32_t levelCount;
+  uint32_t largeStart, largeCount;
+  uint32_t pad2[3];
+};
+
+constexpr int kMaxDepth = 32;   // TreeKernels.cuh:29
+constexpr int kLevelSlots = 34; // depths 0..32 plus an end slot
+
+// Everything a step's kernels touch.  All pointers are device pointers.
+struct DevState {
+  uint32_t n;     // bodies over all segments
+  uint32_t nseg;  // segments
+  uint32_t nodeCapacity;
+  uint32_t pairCapacity;
+  float dt, tSq, eSq;
+  int leafCapacity;
+  int collisions;
+
+  SegDev *seg;
+  uint16_t *segOf; // segment of each body index (never permuted)
+
+  // body state, current order (double-buffered across the Morton gather)
+  float4 *pv;   // {x, y, vx, vy}
+  float2 *mr;   // {mass, radius}
+  uint32_t *id; // Body::id
+  float4 *pv2;
+  float2 *mr2;
+  uint32_t *id2;
+  float2 *acc;  // accelerations from the last force pass
+  float4 *xym;  // {x, y, mass, 0} in Morton order (tree + forces)
+
+  // bounds as float order keys: [seg][minX, maxX, minY, maxY]
+  uint32_t *bounds;
+  uint32_t *status; // error bits
+
+  // collision scratch
+  float4 *box;           // {minX, maxX, minY, maxY}
+  int2 *cellXY;          // grid cell of small boxes
+  uint32_t *slot;        // slot in bucket (small) or in large list (|bit31)
+  uint32_t *bucketCount; // [buckets]
+  uint32_t *bucketStart; // [buckets+1]
+  uint32_t *grid;        // body index per bucket slot
+  uint32_t nBuckets;     // power of two
+  uint32_t *largeCount;  // [nseg]
+  uint32_t *largeStartA; // [nseg]
+  uint32_t *largeList;   // [n]
+  uint32_t *deg;         // partners per body
+  uint32_t *pstart;      // CSR start per body
+  uint32_t *plist;       // partner indices
+  uint32_t *plistTmp;    // scratch copy used to sort large bodies' lists
+  uint32_t *fillLarge;   // fill counters of large bodies
+  uint32_t *nLater;      // partners that sort before the body
+  uint32_t *unitFlag;    // nLater > 0
+  uint32_t *unitPos;     // scan of unitFlag
+  uint32_t *prog;        // resolved chain entries per body
+  uint32_t *unitOrder;   // units in before() order (last collide)
+  uint32_t *counters;    // [0]=pairs*2 total [1]=units [2]=unit claim
+                         // [3]=splitting entries [4]=total nodes
+
+  // Morton / sort
+  uint64_t *codes; // unsorted codes (kept for the segment passes)
+  uint32_t *perm;  // Morton permutation of the last build (sorted -> old)
+  uint64_t *sortedCodes;
+
+  // tree build
+  uint32_t *splitCount; // per body
+  uint32_t *splitStart;
+  uint8_t *splitLo;
+  uint32_t *groupStart; // [nseg][kLevelSlots]
+  uint32_t *groupEnd;
+  uint32_t *levelStart; // [nseg][kLevelSlots+1]
+  // BFS-numbered node arrays (TreeKernels.cuh NodeArrays layout)
+  float *comX, *comY, *mass, *centerX, *centerY, *size;
+  int32_t *children, *next, *start, *end;
+  int32_t *parent;
+  float *sumX, *sumY;   // raw weighted sums (before the CoM divide)
+  float4 *moments;      // {Ixx, Iyy, Ixy, spare}
+  uint32_t *subtree;    // nodes in subtree
+  uint32_t *arrive;     // bottom-up arrival counters
+  // traversal layout (preorder)
+  float4 *tA; // {comX, comY, mass, size*size}
+  int4 *tB;   // {next (preorder, global), start, end, isLeaf}
+  float4 *tM; // {Ixx, Iyy, Ixy, size} for the learned correction
+};
+
+} // namespace nbx

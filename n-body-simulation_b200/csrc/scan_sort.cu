@@ -1,0 +1,360 @@
+// scan_sort.cu -- single-pass exclusive scan and onesweep LSD radix sort.
+//
+// Both use decoupled look-back (Merrill & Garland 2016; Adinets & Merrill
+// 2022, "Onesweep"): tiles are claimed in order through an atomic
+// counter, each tile publishes its aggregate, and looks back over its
+// predecessors' published words until it finds an inclusive prefix.  Every
+// wait is bounded (kSpinLimit); on expiry the kernel raises
+// kStatusSpinLimit in the caller's status word and carries on with what it
+// has, so a stuck predecessor can never hang the GPU.
+//
+// The radix sort is stable (ranks within a warp come from __match_any_sync
+// over warp-striped items, in input order), so equal keys keep their input
+// order exactly as cub::DeviceRadixSort::SortPairs does
+// (CudaQuadTree.cu:405-407), which the Morton permutation parity needs.
+#include "nbx_internal.cuh"
+
+namespace nbx {
+
+// ------------------------------------------------------------------ scan
+namespace {
+
+constexpr uint64_t kFlagShift = 62;
+constexpr uint64_t kValueMask = (1ull << 62) - 1;
+constexpr uint64_t kFlagAgg = 1ull << kFlagShift;
+constexpr uint64_t kFlagIncl = 2ull << kFlagShift;
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
+           uint32_t n_max, const uint32_t *d_n, uint32_t *total,
+           uint64_t *status, uint32_t *tileCounter, uint32_t *err) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_items[kScanTile];
+  __shared__ uint32_t s_warp[kScanThreads / 32];
+  __shared__ uint64_t s_excl;
+  const int tid = threadIdx.x;
+  const uint32_t n = load_count(d_n, n_max);
+  const uint32_t numTiles = (n + kScanTile - 1) / kScanTile;
+  if (tid == 0) s_tile = atomicAdd(tileCounter, 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  if (n == 0) {
+    if (tile == 0 && tid == 0 && total) *total = 0;
+    return;
+  }
+  if (tile >= numTiles) return;
+  const uint32_t base = tile * kScanTile;
+  // striped, coalesced load into shared memory
+  for (int k = 0; k < kScanItems; ++k) {
+    const uint32_t i = base + k * kScanThreads + tid;
+    s_items[k * kScanThreads + tid] = i < n ? in[i] : 0u;
+  }
+  __syncthreads();
+  // blocked read: thread tid owns items [tid*16, tid*16+16)
+  uint32_t v[kScanItems];
+  uint32_t sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = s_items[tid * kScanItems + k];
+    sum += v[k];
+  }
+  // warp inclusive scan of per-thread sums
+  const int lane = tid & 31, warp = tid >> 5;
+  uint32_t inc = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < kScanThreads / 32 ? s_warp[lane] : 0u;
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    const uint32_t blockTotal = __shfl_sync(0xffffffffu, wi, kScanThreads / 32 - 1);
+    if (lane < kScanThreads / 32) s_warp[lane] = wi - w; // exclusive
+    if (lane == 0) {
+      uint64_t excl = 0;
+      if (tile == 0) {
+        st_relaxed_u64(&status[0], kFlagIncl | (uint64_t)blockTotal);
+      } else {
+        st_relaxed_u64(&status[tile], kFlagAgg | (uint64_t)blockTotal);
+        int64_t pred = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        while (pred >= 0) {
+          const uint64_t s = ld_relaxed_u64(&status[pred]);
+          const uint64_t flag = s >> kFlagShift;
+          if (flag == 0) {
+            if (++spins > kSpinLimit) {
+              atomicOr(err, kStatusSpinLimit);
+              break;
+            }
+            __nanosleep(64);
+            continue;
+          }
+          excl += s & kValueMask;
+          if (flag == 2) break;
+          --pred;
+        }
+        st_relaxed_u64(&status[tile], kFlagIncl | ((excl + blockTotal) & kValueMask));
+      }
+      s_excl = excl;
+      if (total && tile == numTiles - 1) *total = (uint32_t)(excl + blockTotal);
+    }
+  }
+  __syncthreads();
+  uint32_t run = (uint32_t)s_excl + s_warp[warp] + (inc - sum);
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    s_items[tid * kScanItems + k] = run;
+    run += v[k];
+  }
+  __syncthreads();
+  for (int k = 0; k < kScanItems; ++k) {
+    const uint32_t i = base + k * kScanThreads + tid;
+    if (i < n) out[i] = s_items[k * kScanThreads + tid];
+  }
+}
+
+} // namespace
+
+size_t scan_scratch_tiles(uint32_t n_max) {
+  return (n_max + kScanTile - 1) / kScanTile + 1;
+}
+
+void exclusive_scan_u32(cudaStream_t s, const uint32_t *in, uint32_t *out,
+                        uint32_t n_max, const uint32_t *d_n, uint32_t *total,
+                        ScanScratch &sc, uint32_t *err) {
+  const uint32_t tiles = (n_max + kScanTile - 1) / kScanTile;
+  cudaMemsetAsync(sc.status, 0, sizeof(uint64_t) * (tiles + 1), s);
+  cudaMemsetAsync(sc.tileCounter, 0, sizeof(uint32_t), s);
+  k_scan<<<tiles > 0 ? tiles : 1, kScanThreads, 0, s>>>(
+      in, out, n_max, d_n, total, sc.status, sc.tileCounter, err);
+}
+
+// ------------------------------------------------------------ radix sort
+namespace {
+
+constexpr uint32_t kRFlagShift = 30;
+constexpr uint32_t kRValueMask = (1u << 30) - 1;
+
+__global__ void k_radix_hist(const uint64_t *__restrict__ keys, uint32_t n_max,
+                             const uint32_t *d_n, int pass_lo, int passes,
+                             uint32_t *__restrict__ hist) {
+  __shared__ uint32_t sh[8][256];
+  for (int i = threadIdx.x; i < passes * 256; i += blockDim.x)
+    sh[i / 256][i % 256] = 0;
+  __syncthreads();
+  const uint32_t n = load_count(d_n, n_max);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    for (int p = 0; p < passes; ++p)
+      atomicAdd(&sh[p][(k >> (8 * (pass_lo + p))) & 255u], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
+    const uint32_t v = sh[i / 256][i % 256];
+    if (v) atomicAdd(&hist[(pass_lo + i / 256) * 256 + i % 256], v);
+  }
+}
+
+// hist[p][*] -> exclusive digit starts, in place.
+__global__ void k_radix_hist_scan(uint32_t *hist, int pass_lo) {
+  __shared__ uint32_t s[256];
+  uint32_t *h = hist + (pass_lo + blockIdx.x) * 256;
+  const int t = threadIdx.x;
+  s[t] = h[t];
+  __syncthreads();
+  for (int o = 1; o < 256; o <<= 1) {
+    const uint32_t v = t >= o ? s[t - o] : 0u;
+    __syncthreads();
+    s[t] += v;
+    __syncthreads();
+  }
+  h[t] = s[t] - h[t];
+}
+
+template <bool kIdentity>
+__global__ void __launch_bounds__(kSortThreads)
+    k_onesweep(const uint64_t *__restrict__ keysIn,
+               const uint32_t *__restrict__ valsIn,
+               uint64_t *__restrict__ keysOut, uint32_t *__restrict__ valsOut,
+               const uint32_t *__restrict__ digitStart, uint32_t *status,
+               uint32_t *tileCounter, uint32_t n_max, const uint32_t *d_n,
+               int shift, uint32_t *err) {
+  __shared__ uint64_t s_keys[kSortTile];
+  __shared__ uint32_t s_vals[kSortTile];
+  __shared__ uint32_t s_whist[kSortWarps][256];
+  __shared__ uint32_t s_local[256];  // local exclusive digit start in tile
+  __shared__ uint32_t s_global[256]; // global start of digit for this tile
+  __shared__ uint32_t s_tile;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t n = load_count(d_n, n_max);
+  const uint32_t numTiles = (n + kSortTile - 1) / kSortTile;
+  if (tid == 0) s_tile = atomicAdd(tileCounter, 1u);
+  for (int i = tid; i < kSortWarps * 256; i += kSortThreads)
+    s_whist[i / 256][i % 256] = 0;
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  if (tile >= numTiles) return;
+  const uint32_t base = tile * kSortTile;
+  const uint32_t wbase = base + warp * (kSortItems * 32);
+
+  uint64_t key[kSortItems];
+  uint32_t val[kSortItems];
+  uint32_t rank[kSortItems];
+  uint32_t dig[kSortItems];
+#pragma unroll
+  for (int k = 0; k < kSortItems; ++k) {
+    const uint32_t i = wbase + k * 32 + lane;
+    const bool ok = i < n;
+    key[k] = ok ? keysIn[i] : 0ull;
+    val[k] = ok ? (kIdentity ? i : valsIn[i]) : 0u;
+    dig[k] = ok ? (uint32_t)((key[k] >> shift) & 255u) : 256u;
+  }
+  const uint32_t ltmask = lanemask_lt();
+#pragma unroll
+  for (int k = 0; k < kSortItems; ++k) {
+    const uint32_t d = dig[k];
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t before = __popc(peers & ltmask);
+    uint32_t b = 0;
+    if (d < 256u) b = s_whist[warp][d];
+    __syncwarp();
+    if (d < 256u && before == 0) s_whist[warp][d] = b + __popc(peers);
+    __syncwarp();
+    rank[k] = b + before;
+  }
+  __syncthreads();
+  // per-digit: warp-exclusive prefixes and the tile count
+  {
+    const int d = tid; // kSortThreads == 256
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) {
+      const uint32_t c = s_whist[w][d];
+      s_whist[w][d] = run;
+      run += c;
+    }
+    const uint32_t count = run;
+    // look-back for this digit
+    uint32_t excl = 0;
+    uint32_t *my = status + (size_t)tile * 256 + d;
+    if (tile == 0) {
+      st_relaxed_u32(my, (2u << kRFlagShift) | count);
+    } else {
+      st_relaxed_u32(my, (1u << kRFlagShift) | count);
+      int pred = (int)tile - 1;
+      uint32_t spins = 0;
+      while (pred >= 0) {
+        const uint32_t s = ld_relaxed_u32(status + (size_t)pred * 256 + d);
+        const uint32_t flag = s >> kRFlagShift;
+        if (flag == 0) {
+          if (++spins > kSpinLimit) {
+            atomicOr(err, kStatusSpinLimit);
+            break;
+          }
+          __nanosleep(32);
+          continue;
+        }
+        excl += s & kRValueMask;
+        if (flag == 2) break;
+        --pred;
+      }
+      st_relaxed_u32(my, (2u << kRFlagShift) | ((excl + count) & kRValueMask));
+    }
+    s_global[d] = digitStart[d] + excl;
+    s_local[d] = count;
+  }
+  __syncthreads();
+  // exclusive scan of tile counts over digits (256 entries, one per thread)
+  {
+    const uint32_t c = s_local[tid];
+    uint32_t inc = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    __shared__ uint32_t s_wsum[kSortWarps];
+    if (lane == 31) s_wsum[warp] = inc;
+    __syncthreads();
+    uint32_t off = 0;
+    for (int w = 0; w < warp; ++w) off += s_wsum[w];
+    __syncthreads();
+    s_local[tid] = off + inc - c;
+  }
+  __syncthreads();
+  // local reorder by digit (stable)
+#pragma unroll
+  for (int k = 0; k < kSortItems; ++k) {
+    const uint32_t d = dig[k];
+    if (d < 256u) {
+      const uint32_t p = s_local[d] + s_whist[warp][d] + rank[k];
+      s_keys[p] = key[k];
+      s_vals[p] = val[k];
+    }
+  }
+  __syncthreads();
+  const uint32_t valid = min((uint32_t)kSortTile, n - base);
+  for (uint32_t p = tid; p < valid; p += kSortThreads) {
+    const uint64_t k = s_keys[p];
+    const uint32_t d = (uint32_t)((k >> shift) & 255u);
+    const uint32_t dest = s_global[d] + (p - s_local[d]);
+    keysOut[dest] = k;
+    valsOut[dest] = s_vals[p];
+  }
+}
+
+} // namespace
+
+size_t sort_tiles(uint32_t n_max) {
+  return (n_max + kSortTile - 1) / kSortTile + 1;
+}
+
+void radix_histogram(cudaStream_t s, SortScratch &sc, const uint64_t *keys,
+                     uint32_t n_max, const uint32_t *d_n, int bit_lo,
+                     int bit_hi) {
+  const int p0 = bit_lo / 8, np = (bit_hi - bit_lo) / 8;
+  cudaMemsetAsync(sc.hist + p0 * 256, 0, sizeof(uint32_t) * 256 * np, s);
+  int blocks = (int)((n_max + 1023) / 1024);
+  if (blocks > 1184) blocks = 1184;
+  if (blocks < 1) blocks = 1;
+  k_radix_hist<<<blocks, 256, 0, s>>>(keys, n_max, d_n, p0, np, sc.hist);
+}
+
+int radix_sort_u64(cudaStream_t s, SortScratch &sc, uint32_t n_max,
+                   const uint32_t *d_n, int bit_lo, int bit_hi,
+                   bool vals_identity, bool have_hist, uint32_t *err) {
+  const int p0 = bit_lo / 8, np = (bit_hi - bit_lo) / 8;
+  if (!have_hist) radix_histogram(s, sc, sc.keys[0], n_max, d_n, bit_lo, bit_hi);
+  k_radix_hist_scan<<<np, 256, 0, s>>>(sc.hist, p0);
+  const uint32_t tiles = (n_max + kSortTile - 1) / kSortTile;
+  cudaMemsetAsync(sc.tileCounter, 0, sizeof(uint32_t) * 8, s);
+  int cur = 0;
+  for (int p = 0; p < np; ++p) {
+    cudaMemsetAsync(sc.status, 0, sizeof(uint32_t) * 256 * (tiles + 1), s);
+    const int shift = 8 * (p0 + p);
+    if (p == 0 && vals_identity) {
+      k_onesweep<true><<<tiles > 0 ? tiles : 1, kSortThreads, 0, s>>>(
+          sc.keys[cur], sc.vals[cur], sc.keys[cur ^ 1], sc.vals[cur ^ 1],
+          sc.hist + (p0 + p) * 256, sc.status, sc.tileCounter + p, n_max, d_n,
+          shift, err);
+    } else {
+      k_onesweep<false><<<tiles > 0 ? tiles : 1, kSortThreads, 0, s>>>(
+          sc.keys[cur], sc.vals[cur], sc.keys[cur ^ 1], sc.vals[cur ^ 1],
+          sc.hist + (p0 + p) * 256, sc.status, sc.tileCounter + p, n_max, d_n,
+          shift, err);
+    }
+    cur ^= 1;
+  }
+  return cur;
+}
+
+} // namespace nbx

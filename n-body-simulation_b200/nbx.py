@@ -1,0 +1,281 @@
+"""Python binding of the C ABI in include/nbx.h (ctypes over lib/libnbx.so).
+
+The library is the product: this module only marshals numpy arrays in and
+out.  It raises if the shared library is missing -- there is no fallback.
+
+    sim = Simulation(nbx.uniform_disc(10000))   # one instance
+    sim.step(100)
+    bodies = sim.download(id_order=True)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libnbx.so")
+
+BODY_DTYPE = np.dtype([
+    ("px", "<f4"), ("py", "<f4"), ("vx", "<f4"), ("vy", "<f4"),
+    ("ax", "<f4"), ("ay", "<f4"), ("mass", "<f4"), ("radius", "<f4"),
+    ("id", "<u4"),
+])
+assert BODY_DTYPE.itemsize == 36
+
+# Every entry point declared in include/nbx.h.
+EXPORTS = (
+    "nbx_params_default", "nbx_create", "nbx_destroy", "nbx_set_params",
+    "nbx_get_params", "nbx_upload_bodies", "nbx_download_bodies", "nbx_step",
+    "nbx_sync", "nbx_phase", "nbx_get_morton", "nbx_tree_size", "nbx_get_tree",
+    "nbx_get_pairs", "nbx_direct_fp64", "nbx_force_error_fp64",
+    "nbx_energy_momentum_fp64", "nbx_status_bits", "nbx_last_error",
+    "nbx_uniform_disc", "nbx_two_discs", "nbx_cold_square", "nbx_version",
+)
+
+PHASE = {"iterate": 0, "collide": 1, "build": 2, "forces": 3, "attract": 4,
+         "step": 5}
+ERRORS = {1: "NBX_ERR_ARG", 2: "NBX_ERR_CUDA", 3: "NBX_ERR_CAPACITY",
+          4: "NBX_ERR_NONFINITE", 5: "NBX_ERR_TIMEOUT", 6: "NBX_ERR_STATE",
+          7: "NBX_ERR_NOMEM"}
+
+
+class Params(C.Structure):
+    _fields_ = [("dt", C.c_float), ("theta", C.c_float), ("epsilon", C.c_float),
+                ("leaf_capacity", C.c_int32), ("collisions", C.c_int32),
+                ("exact_math", C.c_int32), ("use_mlp", C.c_int32),
+                ("node_factor", C.c_float), ("pair_factor", C.c_float),
+                ("force_blocks", C.c_int32)]
+
+
+class NbxError(RuntimeError):
+    def __init__(self, code, msg=""):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(
+            f"{LIB_PATH} is missing: build it with `make -C {HERE}` "
+            "(there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+    u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+    i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+    f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+    bodyp = np.ctypeslib.ndpointer(BODY_DTYPE, flags="C_CONTIGUOUS")
+    sig = {
+        "nbx_params_default": [C.POINTER(Params)],
+        "nbx_create": [C.POINTER(Params), C.c_uint32, u32p, C.POINTER(vp)],
+        "nbx_destroy": [vp],
+        "nbx_set_params": [vp, C.POINTER(Params)],
+        "nbx_get_params": [vp, C.POINTER(Params)],
+        "nbx_upload_bodies": [vp, vp, C.c_size_t],
+        "nbx_download_bodies": [vp, vp, C.c_size_t, C.c_int],
+        "nbx_step": [vp, C.c_uint32],
+        "nbx_sync": [vp],
+        "nbx_phase": [vp, C.c_int],
+        "nbx_get_morton": [vp, C.c_uint32, u64p, u32p, C.c_size_t],
+        "nbx_tree_size": [vp, C.c_uint32, C.POINTER(C.c_uint32),
+                          C.POINTER(C.c_uint32)],
+        "nbx_get_tree": [vp, C.c_uint32] + [vp] * 10 + [C.c_size_t],
+        "nbx_get_pairs": [vp, i32p, i32p, C.c_int64, C.POINTER(C.c_int64)],
+        "nbx_direct_fp64": [vp, u32p, C.c_uint32, f64p, f64p],
+        "nbx_force_error_fp64": [vp, u32p, C.c_uint32, f64p, vp],
+        "nbx_energy_momentum_fp64": [vp, f64p],
+        "nbx_status_bits": [vp, C.POINTER(C.c_uint32)],
+        "nbx_last_error": [vp],
+        "nbx_uniform_disc": [C.c_uint32, C.c_uint32, bodyp],
+        "nbx_two_discs": [C.c_uint32, C.c_uint32, C.c_float, bodyp],
+        "nbx_cold_square": [C.c_uint32, C.c_uint32, bodyp],
+        "nbx_version": [],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    L.nbx_last_error.restype = C.c_char_p
+    L.nbx_version.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    lib().nbx_params_default(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def uniform_disc(n: int, seed: int = 0) -> np.ndarray:
+    b = np.zeros(n, BODY_DTYPE)
+    _check(None, lib().nbx_uniform_disc(n, seed, b))
+    return b
+
+
+def two_discs(n: int, seed: int = 0, approach: float = 0.2) -> np.ndarray:
+    b = np.zeros(n, BODY_DTYPE)
+    _check(None, lib().nbx_two_discs(n, seed, approach, b))
+    return b
+
+
+def cold_square(n: int, seed: int = 0) -> np.ndarray:
+    b = np.zeros(n, BODY_DTYPE)
+    _check(None, lib().nbx_cold_square(n, seed, b))
+    return b
+
+
+def _check(h, rc):
+    if rc != 0:
+        msg = lib().nbx_last_error(h).decode() if h else ""
+        raise NbxError(rc, msg)
+
+
+class Handle:
+    """One nbx handle: one or more instances advanced together."""
+
+    def __init__(self, sizes, params: Params | None = None, **kw):
+        self.sizes = np.ascontiguousarray(np.atleast_1d(sizes), np.uint32)
+        self.n = int(self.sizes.sum())
+        self.starts = np.concatenate([[0], np.cumsum(self.sizes)[:-1]]).astype(np.int64)
+        p = params if params is not None else default_params(**kw)
+        h = C.c_void_p()
+        _check(None, lib().nbx_create(C.byref(p), len(self.sizes), self.sizes,
+                                      C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().nbx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _c(self, rc):
+        _check(self.h, rc)
+
+    @property
+    def params(self) -> Params:
+        p = Params()
+        self._c(lib().nbx_get_params(self.h, C.byref(p)))
+        return p
+
+    def set_params(self, **kw):
+        p = self.params
+        for k, v in kw.items():
+            setattr(p, k, v)
+        self._c(lib().nbx_set_params(self.h, C.byref(p)))
+
+    def upload(self, bodies: np.ndarray):
+        b = np.ascontiguousarray(bodies, BODY_DTYPE)
+        self._c(lib().nbx_upload_bodies(self.h, b.ctypes.data, len(b)))
+
+    def upload_ptr(self, ptr: int, n: int):
+        self._c(lib().nbx_upload_bodies(self.h, ptr, n))
+
+    def download(self, id_order: bool = False, out: np.ndarray | None = None):
+        if out is None:
+            out = np.zeros(self.n, BODY_DTYPE)
+        self._c(lib().nbx_download_bodies(self.h, out.ctypes.data, self.n,
+                                          int(id_order)))
+        return out
+
+    def download_ptr(self, ptr: int, n: int, id_order: bool = False):
+        self._c(lib().nbx_download_bodies(self.h, ptr, n, int(id_order)))
+
+    def step(self, steps: int = 1):
+        self._c(lib().nbx_step(self.h, steps))
+
+    def sync(self):
+        self._c(lib().nbx_sync(self.h))
+
+    def phase(self, name: str):
+        self._c(lib().nbx_phase(self.h, PHASE[name]))
+
+    def morton(self, instance: int = 0):
+        m = int(self.sizes[instance])
+        codes = np.zeros(m, np.uint64)
+        perm = np.zeros(m, np.uint32)
+        self._c(lib().nbx_get_morton(self.h, instance, codes, perm, m))
+        return codes, perm
+
+    def tree(self, instance: int = 0) -> dict:
+        nodes, levels = C.c_uint32(), C.c_uint32()
+        self._c(lib().nbx_tree_size(self.h, instance, C.byref(nodes),
+                                    C.byref(levels)))
+        c = nodes.value
+        out = {k: np.zeros(c, np.float32) for k in
+               ("comX", "comY", "mass", "centerX", "centerY", "size")}
+        out.update({k: np.zeros(c, np.int32) for k in
+                    ("children", "next", "start", "end")})
+        order = ("comX", "comY", "mass", "centerX", "centerY", "size",
+                 "children", "next", "start", "end")
+        self._c(lib().nbx_get_tree(self.h, instance,
+                                   *[out[k].ctypes.data for k in order], c))
+        out["node_count"] = c
+        out["level_count"] = levels.value
+        return out
+
+    def pairs(self):
+        cnt = C.c_int64()
+        empty = np.zeros(1, np.int32)
+        self._c(lib().nbx_get_pairs(self.h, empty, empty, 0, C.byref(cnt)))
+        k = cnt.value
+        later = np.zeros(max(k, 1), np.int32)
+        earlier = np.zeros(max(k, 1), np.int32)
+        self._c(lib().nbx_get_pairs(self.h, later, earlier, k, C.byref(cnt)))
+        return later[:k], earlier[:k]
+
+    def direct_fp64(self, targets):
+        t = np.ascontiguousarray(targets, np.uint32)
+        ax = np.zeros(len(t), np.float64)
+        ay = np.zeros(len(t), np.float64)
+        self._c(lib().nbx_direct_fp64(self.h, t, len(t), ax, ay))
+        return ax, ay
+
+    def force_error(self, targets):
+        t = np.ascontiguousarray(targets, np.uint32)
+        stats = np.zeros(4, np.float64)
+        err = np.zeros(len(t), np.float64)
+        self._c(lib().nbx_force_error_fp64(self.h, t, len(t), stats,
+                                           err.ctypes.data))
+        return {"median": stats[0], "p99": stats[1], "max": stats[2],
+                "mean": stats[3]}, err
+
+    def energy_momentum(self):
+        out = np.zeros(5, np.float64)
+        self._c(lib().nbx_energy_momentum_fp64(self.h, out))
+        return out
+
+    def status_bits(self) -> int:
+        b = C.c_uint32()
+        self._c(lib().nbx_status_bits(self.h, C.byref(b)))
+        return b.value
+
+
+class Simulation(Handle):
+    """One simulation: the reference's Simulation / CudaSimulation."""
+
+    def __init__(self, bodies: np.ndarray, **kw):
+        super().__init__([len(bodies)], **kw)
+        self.upload(bodies)
