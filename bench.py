@@ -1,0 +1,333 @@
+"""Benchmark of the B200 Simulation::step path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (the headline configuration): two rotating discs of 2^19 bodies
+each (1,048,576 total), centres 6R apart on x, bulk velocities +-0.2 of the
+circular speed on y, opposite spins; FP32; theta = 0.5, epsilon = 1,
+dt = 0.05, leaf capacity 16, collisions on.  A "step" is one
+Simulation::step (iterate -> collide -> tree build -> forces) of that
+system.  Inputs are synthetic (the reference uses no dataset).
+
+value: body-steps/s with the state resident in HBM, timed with CUDA events
+on the library's stream over K steps (one captured graph per step),
+barrier + synchronize on both sides, max over ranks.  With N GPUs each rank
+advances its own replica (the single simulation does not shard), so the
+whole-job value is N x bodies / step time ("scaling": "weak").
+
+e2e: the same metric through the C ABI as a drop-in Simulation::step with a
+host-owned body array: per step the 36-byte Body records go host -> device
+(pinned), one step runs, and they come back device -> host.
+
+--impl reference times the reference's own OpenMP CPU implementation
+(oracle/_ref/libref_omp.so, built from the reference's sources with its own
+flags) on the same workload; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "n-body-simulation_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "body-steps/s at 1M: plain vs learned-theta at equal FP64 force error; ensemble"
+UNIT = "body-steps/s"
+N_BODIES = 1 << 20
+THETA = 0.5
+WORKLOAD = {
+    "workload": "two discs 2x2^19 bodies (1,048,576), centres 6R apart, "
+                "+-0.2 v_circ bulk, opposite spin; theta 0.5, eps 1, dt 0.05, "
+                "leaf 16, collisions on",
+    "bodies": N_BODIES, "theta": THETA, "epsilon": 1.0, "dt": 0.05,
+    "leaf_capacity": 16, "collisions": True,
+    "l2": "no flush: the per-step working set (~0.3 GB) exceeds the 126 MB L2",
+}
+# Algorithmic FLOPs per interaction (GPU Gems 3 ch. 31 convention).
+FLOP_PER_INTERACTION = 20.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=N_BODIES)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200", "-i",
+                 str(self.gpu)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------ distributed
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local, dist
+
+
+def max_over_ranks(dist, local, v: float) -> float:
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ------------------------------------------------------------- reference
+def reference_rate(n, steps, warmup, bodies=None):
+    """The reference's OpenMP Simulation::step (its own flags), all cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Reference
+    R = Reference("omp")
+    import nbx
+    b = bodies if bodies is not None else nbx.two_discs(n, 0, 0.2)
+    if warmup:
+        b, _ = R.simulate(b, theta=THETA, steps=warmup)
+    _, ms = R.simulate(b, theta=THETA, steps=steps)
+    return n * steps / (ms * 1e-3), R.threads(), ms / steps
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 20))
+    warm = max(1, min(args.warmup, 2))
+    value, cores, ms = reference_rate(args.n, steps, warm)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": warm, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "config": WORKLOAD,
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores,
+                         "kind": "reference",
+                         "sample": f"{steps} Simulation::step calls of the "
+                                   f"{args.n}-body workload after {warm} warm-up "
+                                   "steps (requested steps capped at 20)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ b200
+def run_b200(args):
+    world, rank, local, dist = dist_setup(args)
+    import torch
+    torch.cuda.set_device(local)
+    import nbx
+    n = args.n
+    bodies = nbx.two_discs(n, 0, 0.2)
+    sim = nbx.Simulation(bodies, theta=THETA, device=local)
+    stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+
+    sim.step(args.warmup)
+    sim.sync()
+    kernels_per_step = sim.step_kernels()
+
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        barrier(dist)
+        torch.cuda.synchronize(local)
+        sim.sync()
+        e0.record(stream)
+        sim.step(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        sim.sync()
+        torch.cuda.synchronize(local)
+        barrier(dist)
+    ms_rank = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(dist, local, ms_rank)
+    value = world * n / (ms * 1e-3)
+
+    # dominant kernel: the force traversal, timed alone on the same stream
+    inter = sim.interactions()
+    reps = 5
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    sim.phase("forces")
+    f0.record(stream)
+    for _ in range(reps):
+        sim.phase("forces")
+    f1.record(stream)
+    f1.synchronize()
+    force_ms = f0.elapsed_time(f1) / reps
+    flops = FLOP_PER_INTERACTION * (inter["far"] + inter["near"])
+    achieved = flops / (force_ms * 1e-3) / 1e12
+    peak = nbx.fp32_peak_tflops()
+
+    # force error against the FP64 direct sum on 4096 sampled bodies
+    s = sim.download()
+    rng = np.random.default_rng(12345)
+    ids = rng.choice(n, 4096, replace=False)
+    pos = np.empty(n, np.int64)
+    pos[s["id"]] = np.arange(n)
+    err_stats, _ = sim.force_error(pos[ids].astype(np.uint32))
+
+    # e2e: host-owned bodies, H2D + step + D2H every step
+    e2e_steps = max(3, min(args.steps, 100))
+    host = torch.empty(n * 36, dtype=torch.uint8, pin_memory=True)
+    hb = host.numpy().view(nbx.BODY_DTYPE)
+    hb[:] = s
+    ptr = host.data_ptr()
+    sim.upload_ptr(ptr, n)
+    sim.step(1)
+    sim.download_ptr(ptr, n)
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    barrier(dist)
+    t0 = time.perf_counter()
+    g0.record(stream)
+    for _ in range(e2e_steps):
+        sim.upload_ptr(ptr, n)
+        sim.step(1)
+        sim.download_ptr(ptr, n)
+    g1.record(stream)
+    g1.synchronize()
+    wall = time.perf_counter() - t0
+    e2e_ms = max(g0.elapsed_time(g1), wall * 1e3) / e2e_steps
+    e2e_ms = max_over_ranks(dist, local, e2e_ms)
+    e2e_value = world * n / (e2e_ms * 1e-3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, cores, cms = reference_rate(n, 8, 1, bodies)
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                   "sample": f"8 Simulation::step calls of the same {n}-body "
+                             f"workload after 1 warm-up step ({cms:.0f} ms/step), "
+                             "reference built with its own flags (-Ofast -fopenmp)"}
+        except Exception as ex:  # reference build absent
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {ex}"}
+
+    clk = clocks.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": dict(WORKLOAD, parallelism=f"replicas{world}" if world > 1 else "single"),
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": 36 * n, "d2h_bytes_per_step": 36 * n,
+                "ms_per_step": e2e_ms},
+        "roofline": {
+            "kernel": "k_forces (warp-cooperative traversal)",
+            "bound": "fp32", "achieved": achieved, "peak": peak,
+            "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+            "traffic": None,
+            "peak_note": "FP32 FMA peak measured live by a probe kernel "
+                         "(MEASURED_PEAKS.json holds no FP32 figure)",
+            "flops_per_launch": flops, "launch_ms": force_ms,
+            "interactions_per_body": (inter["far"] + inter["near"]) / n,
+        },
+        "force_error_fp64": {"p50": err_stats["median"], "p99": err_stats["p99"],
+                             "max": err_stats["max"], "samples": 4096},
+        "interactions_per_s": (inter["far"] + inter["near"]) * 1e3 / ms,
+        "gpu_launches": kernels_per_step * args.steps,
+        "clocks": clk,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -65,6 +65,7 @@ typedef struct nbx_params {
                              reference bound 8n+8, CudaQuadTree.cu:270-273) */
   float pair_factor;      /* collision partner slots per body (default 32) */
   int32_t force_blocks;   /* 0 = auto; else blocks of the force launch */
+  int32_t device;         /* CUDA device ordinal; -1 = the current device */
 } nbx_params;
 
 typedef struct nbx_handle nbx_handle;
@@ -169,6 +170,30 @@ int nbx_force_error_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m,
 /* Compensated FP64 sums over all bodies: {kinetic energy, px, py, Lz,
  * total mass}.  No counterpart in the reference. */
 int nbx_energy_momentum_fp64(nbx_handle *h, double *out5);
+
+/* --- measurement helpers (no counterpart in the reference) --- */
+
+/* The CUDA stream (cudaStream_t) all of the handle's work runs on, so that
+ * callers can time it with events recorded on the same stream. */
+int nbx_get_stream(nbx_handle *h, void **stream);
+
+/* Runs one step eagerly with CUDA events between its stages and returns
+ * the stage durations: labels holds max_marks strings of 32 chars, ms the
+ * milliseconds, *count the number of stages. */
+int nbx_profile_step(nbx_handle *h, uint32_t max_marks, char *labels,
+                     float *ms, uint32_t *count);
+
+/* Kernel launches in one captured step. */
+int nbx_step_kernel_count(nbx_handle *h, uint32_t *kernels);
+
+/* Interactions of the traversal over the last tree for every body:
+ * out5 = {accepted nodes with mass > 0, leaf body terms, visited nodes,
+ * warp iterations, node-tile loads}. */
+int nbx_interaction_count(nbx_handle *h, double *out5);
+
+/* FP32 FMA throughput of the current device (TFLOP/s, 2 flops per FMA),
+ * measured with a probe kernel. */
+int nbx_fp32_peak_tflops(double *tflops);
 
 /* Device status bits (cleared on read) and the last error message. */
 int nbx_status_bits(nbx_handle *h, uint32_t *bits);

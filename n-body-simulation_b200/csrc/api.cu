@@ -20,6 +20,9 @@ void launch_bounds(cudaStream_t s, const DevState &S);
 void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
                   SortScratch &sort);
 void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks);
+void launch_interaction_count(cudaStream_t s, const DevState &S,
+                              unsigned long long *counts);
+double fp32_fma_peak_tflops(cudaStream_t s);
 void launch_direct_fp64(cudaStream_t s, const float4 *pv, const float2 *mr,
                         uint32_t n, const uint32_t *targets, uint32_t m,
                         double eps, double2 *partial, double *ax, double *ay);
@@ -27,6 +30,10 @@ size_t direct_partial_elems(uint32_t m);
 void launch_energy_momentum(cudaStream_t s, const float4 *pv, const float2 *mr,
                             uint32_t n, double *part, double *out);
 } // namespace nbx
+
+namespace nbx {
+thread_local PhaseMarks *g_marks = nullptr;
+}
 
 using namespace nbx;
 
@@ -69,6 +76,18 @@ __global__ void k_pack(const float4 *__restrict__ pv, const float2 *__restrict__
   }
 }
 
+__global__ void k_check_ids(const uint32_t *__restrict__ id,
+                            const uint16_t *__restrict__ segOf,
+                            const SegDev *seg, uint32_t n, uint32_t *seen,
+                            uint32_t *bad) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    const SegDev &G = seg[segOf[i]];
+    const uint32_t v = id[i];
+    if (v >= G.count || atomicExch(&seen[G.start + v], 1u) != 0u) *bad = 1u;
+  }
+}
+
 __global__ void k_fill_u16(uint16_t *p, uint32_t start, uint32_t count,
                            uint16_t v) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count;
@@ -95,10 +114,12 @@ struct nbx_handle {
   ScanScratch scan;
   SortScratch sort;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  uint32_t graphKernels = 0; // kernel nodes per captured step
   bool graphsValid = false;
   bool uploaded = false;
   bool treeValid = false;
   bool collideValid = false;
+  bool idsChecked = false;     // ids verified to be per-instance permutations
   bool idsPermutation = false;
   nbx_body *dAoS = nullptr;     // device staging of body records
   nbx_body *hPinned = nullptr;  // pinned host staging
@@ -195,6 +216,7 @@ int allocate(nbx_handle *h) {
   A(S.pstart, n + 1);
   A(S.plist, S.pairCapacity);
   A(S.plistTmp, S.pairCapacity);
+  A(S.twin, S.pairCapacity);
   A(S.fillLarge, n);
   A(S.nLater, n);
   A(S.unitFlag, n);
@@ -296,9 +318,11 @@ DevState enqueue_step(nbx_handle *h, cudaStream_t s, DevState S) {
     cudaMemsetAsync(S.largeCount, 0, sizeof(uint32_t) * S.nseg, s);
   }
   launch_integrate(s, S, true, S.collisions != 0);
+  mark(s, "integrate");
   if (S.collisions) launch_collide(s, S, h->scan, h->sort);
   launch_build(s, S, h->scan, h->sort);
   launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks);
+  mark(s, "forces");
   return S;
 }
 
@@ -322,6 +346,19 @@ int capture_graphs(nbx_handle *h) {
     enqueue_step(h, h->stream, S);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+    if (p == 0) {
+      size_t count = 0;
+      cudaGraphGetNodes(g, nullptr, &count);
+      std::vector<cudaGraphNode_t> nodes(count);
+      cudaGraphGetNodes(g, nodes.data(), &count);
+      uint32_t kernels = 0;
+      for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+          ++kernels;
+      }
+      h->graphKernels = kernels;
+    }
     e = cudaGraphInstantiate(&h->graph[p], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
@@ -370,6 +407,7 @@ int nbx_params_default(nbx_params *p) {
   p->node_factor = 8.0f;
   p->pair_factor = 32.0f;
   p->force_blocks = 0;
+  p->device = -1;
   return NBX_OK;
 }
 
@@ -395,7 +433,9 @@ int nbx_create(const nbx_params *p, uint32_t num, const uint32_t *sizes,
     h->segCount.push_back(sizes[s]);
     run += sizes[s];
   }
-  cudaError_t e = cudaGetDevice(&h->device);
+  cudaError_t e = cudaSuccess;
+  if (P.device >= 0) e = cudaSetDevice(P.device);
+  if (e == cudaSuccess) e = cudaGetDevice(&h->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   int rc = e == cudaSuccess ? allocate(h) : cuda_fail(h, e, "stream");
   if (rc != NBX_OK) {
@@ -410,6 +450,7 @@ int nbx_create(const nbx_params *p, uint32_t num, const uint32_t *sizes,
 
 int nbx_destroy(nbx_handle *h) {
   if (!h) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   destroy_graphs(h);
   for (void *v : h->allocs) cudaFree(v);
@@ -440,6 +481,7 @@ int nbx_get_params(const nbx_handle *h, nbx_params *p) {
 
 int nbx_upload_bodies(nbx_handle *h, const nbx_body *bodies, size_t n) {
   if (!h || (!bodies && n) || n != h->n) return h ? fail(h, NBX_ERR_ARG, "body count mismatch") : NBX_ERR_ARG;
+  cudaSetDevice(h->device);
   if (n == 0) {
     h->uploaded = true;
     return NBX_OK;
@@ -464,23 +506,22 @@ int nbx_upload_bodies(nbx_handle *h, const nbx_body *bodies, size_t n) {
   NBX_CUDA(h, cudaMemcpyAsync(seg.data(), S.seg, h->nseg * sizeof(SegDev),
                               cudaMemcpyDeviceToHost, h->stream));
   NBX_CUDA(h, cudaStreamSynchronize(h->stream));
-  bool perm = true;
+  // The grid cell only sets how the broadphase partitions space: the
+  // candidate set (every overlapping box pair) does not depend on it.  It
+  // is 2 x 1.01 x the median radius of an evenly strided sample of at most
+  // 4096 bodies per instance (CudaCollision.cu:201-215 takes the median of
+  // all radii); deterministic for a given input.
   std::vector<float> radii;
-  std::vector<uint8_t> seen;
   for (uint32_t s = 0; s < h->nseg; ++s) {
     const uint32_t s0 = h->segStart[s], cnt = h->segCount[s];
-    radii.resize(cnt);
-    seen.assign(cnt, 0);
-    for (uint32_t i = 0; i < cnt; ++i) {
-      radii[i] = bodies[s0 + i].radius;
-      const uint32_t id = bodies[s0 + i].id;
-      if (id >= cnt || seen[id]) perm = false;
-      else seen[id] = 1;
-    }
+    const uint32_t stride = cnt > 4096 ? cnt / 4096 : 1;
+    radii.clear();
+    for (uint32_t i = 0; i < cnt; i += stride) radii.push_back(bodies[s0 + i].radius);
     float cell = 1.0f;
-    if (cnt) {
-      std::nth_element(radii.begin(), radii.begin() + cnt / 2, radii.end());
-      cell = 2.0f * radii[cnt / 2] * 1.01f;
+    if (!radii.empty()) {
+      const size_t mid = radii.size() / 2;
+      std::nth_element(radii.begin(), radii.begin() + mid, radii.end());
+      cell = 2.0f * radii[mid] * 1.01f;
     }
     if (!(cell > 0.0f) || !std::isfinite(cell)) cell = 1.0f;
     seg[s].cell = cell;
@@ -490,7 +531,7 @@ int nbx_upload_bodies(nbx_handle *h, const nbx_body *bodies, size_t n) {
   NBX_CUDA(h, cudaMemcpyAsync(S.seg, seg.data(), h->nseg * sizeof(SegDev),
                               cudaMemcpyHostToDevice, h->stream));
   NBX_CUDA(h, cudaStreamSynchronize(h->stream));
-  h->idsPermutation = perm;
+  h->idsChecked = false;
   h->uploaded = true;
   h->treeValid = false;
   h->collideValid = false;
@@ -499,6 +540,22 @@ int nbx_upload_bodies(nbx_handle *h, const nbx_body *bodies, size_t n) {
 
 int nbx_download_bodies(nbx_handle *h, nbx_body *bodies, size_t n, int idOrder) {
   if (!h || (!bodies && n) || n != h->n) return h ? fail(h, NBX_ERR_ARG, "body count mismatch") : NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (idOrder && !h->idsChecked) {
+    // ids must be a permutation of 0..size-1 in every instance; checked on
+    // the device once per upload (steps only permute bodies)
+    const DevState S0 = h->state();
+    uint32_t *seen = S0.splitCount, *bad = S0.counters + 8;
+    NBX_CUDA(h, cudaMemsetAsync(seen, 0, 4ull * h->n, h->stream));
+    NBX_CUDA(h, cudaMemsetAsync(bad, 0, 4, h->stream));
+    k_check_ids<<<std::min<uint32_t>((h->n + 255) / 256, 4096), 256, 0, h->stream>>>(
+        S0.id, S0.segOf, S0.seg, h->n, seen, bad);
+    uint32_t b = 0;
+    NBX_CUDA(h, cudaMemcpyAsync(&b, bad, 4, cudaMemcpyDeviceToHost, h->stream));
+    NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->idsPermutation = b == 0;
+    h->idsChecked = true;
+  }
   if (idOrder && !h->idsPermutation)
     return fail(h, NBX_ERR_ARG, "ids are not a permutation of 0..size-1 per instance");
   if (n == 0) return NBX_OK;
@@ -520,6 +577,7 @@ int nbx_download_bodies(nbx_handle *h, nbx_body *bodies, size_t n, int idOrder) 
 
 int nbx_step(nbx_handle *h, uint32_t steps) {
   if (!h) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
   if (!h->uploaded) return fail(h, NBX_ERR_STATE, "no bodies uploaded");
   if (h->n == 0 || steps == 0) return NBX_OK;
   if (!h->graphsValid) {
@@ -537,12 +595,14 @@ int nbx_step(nbx_handle *h, uint32_t steps) {
 
 int nbx_sync(nbx_handle *h) {
   if (!h) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
   NBX_CUDA(h, cudaStreamSynchronize(h->stream));
   return check_status(h);
 }
 
 int nbx_phase(nbx_handle *h, int phase) {
   if (!h) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
   if (!h->uploaded) return fail(h, NBX_ERR_STATE, "no bodies uploaded");
   if (h->n == 0) return NBX_OK;
   cudaStream_t s = h->stream;
@@ -589,6 +649,7 @@ int nbx_phase(nbx_handle *h, int phase) {
 int nbx_get_morton(nbx_handle *h, uint32_t inst, uint64_t *codes, uint32_t *perm,
                    size_t n) {
   if (!h || inst >= h->nseg || n != h->segCount[inst]) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
   if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
   const uint32_t s0 = h->segStart[inst];
   if (codes)
@@ -610,6 +671,7 @@ static int read_seg(nbx_handle *h, uint32_t inst, SegDev &g) {
 
 int nbx_tree_size(nbx_handle *h, uint32_t inst, uint32_t *nodes, uint32_t *levels) {
   if (!h || inst >= h->nseg) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
   if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
   SegDev g;
   int rc = read_seg(h, inst, g);
@@ -623,6 +685,7 @@ int nbx_get_tree(nbx_handle *h, uint32_t inst, float *comX, float *comY, float *
                  float *cx, float *cy, float *size, int32_t *children, int32_t *next,
                  int32_t *start, int32_t *end, size_t capacity) {
   if (!h || inst >= h->nseg) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
   if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
   SegDev g;
   int rc = read_seg(h, inst, g);
@@ -648,6 +711,7 @@ int nbx_get_tree(nbx_handle *h, uint32_t inst, float *comX, float *comY, float *
 int nbx_get_pairs(nbx_handle *h, int32_t *later, int32_t *earlier, int64_t cap,
                   int64_t *count) {
   if (!h || !count) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
   if (!h->collideValid) return fail(h, NBX_ERR_STATE, "no collide run");
   const DevState &S = h->base;
   const uint32_t n = h->n;
@@ -679,6 +743,7 @@ int nbx_get_pairs(nbx_handle *h, int32_t *later, int32_t *earlier, int64_t cap,
 int nbx_direct_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m, double *ax,
                     double *ay) {
   if (!h || (m && (!targets || !ax || !ay))) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
   if (m == 0) return NBX_OK;
   for (uint32_t k = 0; k < m; ++k)
     if (targets[k] >= h->n) return fail(h, NBX_ERR_ARG, "target index out of range");
@@ -735,6 +800,7 @@ int nbx_force_error_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m,
 
 int nbx_energy_momentum_fp64(nbx_handle *h, double *out5) {
   if (!h || !out5) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
   const DevState S = h->state();
   launch_energy_momentum(h->stream, S.pv, S.mr, h->n, h->dF64, h->dF64 + 10 * 592);
   NBX_CUDA(h, cudaGetLastError());
@@ -745,10 +811,85 @@ int nbx_energy_momentum_fp64(nbx_handle *h, double *out5) {
 
 int nbx_status_bits(nbx_handle *h, uint32_t *bits) {
   if (!h || !bits) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
   NBX_CUDA(h, cudaMemcpyAsync(bits, h->base.status, 4, cudaMemcpyDeviceToHost, h->stream));
   NBX_CUDA(h, cudaMemsetAsync(h->base.status, 0, 4, h->stream));
   NBX_CUDA(h, cudaStreamSynchronize(h->stream));
   return NBX_OK;
+}
+
+int nbx_profile_step(nbx_handle *h, uint32_t max_marks, char *labels,
+                     float *ms, uint32_t *count) {
+  if (!h || !count || (max_marks && (!labels || !ms))) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!h->uploaded) return fail(h, NBX_ERR_STATE, "no bodies uploaded");
+  PhaseMarks marks;
+  for (int k = 0; k < PhaseMarks::kMax; ++k) cudaEventCreate(&marks.ev[k]);
+  cudaStream_t s = h->stream;
+  g_marks = &marks;
+  mark(s, "start");
+  enqueue_step(h, s, h->state());
+  g_marks = nullptr;
+  h->cur ^= 1;
+  h->treeValid = true;
+  h->collideValid = h->params.collisions != 0;
+  cudaError_t e = cudaStreamSynchronize(s);
+  const uint32_t segs = marks.count > 0 ? (uint32_t)marks.count - 1 : 0;
+  *count = segs;
+  for (uint32_t k = 0; k < segs && k < max_marks; ++k) {
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, marks.ev[k], marks.ev[k + 1]);
+    ms[k] = t;
+    std::snprintf(labels + 32 * k, 32, "%s", marks.label[k + 1]);
+  }
+  for (int k = 0; k < PhaseMarks::kMax; ++k) cudaEventDestroy(marks.ev[k]);
+  if (e != cudaSuccess) return cuda_fail(h, e, "profile step");
+  return check_status(h);
+}
+
+int nbx_get_stream(nbx_handle *h, void **stream) {
+  if (!h || !stream) return NBX_ERR_ARG;
+  *stream = (void *)h->stream;
+  return NBX_OK;
+}
+
+int nbx_step_kernel_count(nbx_handle *h, uint32_t *kernels) {
+  if (!h || !kernels) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!h->graphsValid) {
+    if (!h->uploaded) return fail(h, NBX_ERR_STATE, "no bodies uploaded");
+    int rc = capture_graphs(h);
+    if (rc) return rc;
+  }
+  *kernels = h->graphKernels;
+  return NBX_OK;
+}
+
+int nbx_interaction_count(nbx_handle *h, double *out5) {
+  // out3 holds 5 entries: far, near, visits, warp iterations, tile loads
+  if (!h || !out5) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
+  const DevState S = h->state();
+  unsigned long long *d = reinterpret_cast<unsigned long long *>(h->dF64 + 15 * 592);
+  launch_interaction_count(h->stream, S, d);
+  NBX_CUDA(h, cudaGetLastError());
+  unsigned long long c[5];
+  NBX_CUDA(h, cudaMemcpyAsync(c, d, sizeof c, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (int k = 0; k < 5; ++k) out5[k] = (double)c[k];
+  return NBX_OK;
+}
+
+int nbx_fp32_peak_tflops(double *tflops) {
+  if (!tflops) return NBX_ERR_ARG;
+  cudaStream_t s;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+    return NBX_ERR_CUDA;
+  *tflops = fp32_fma_peak_tflops(s);
+  cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  return *tflops > 0 ? NBX_OK : NBX_ERR_CUDA;
 }
 
 const char *nbx_last_error(const nbx_handle *h) {

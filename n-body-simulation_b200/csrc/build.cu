@@ -502,9 +502,12 @@ void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
   const uint32_t n = S.n;
   launch_bounds(s, S);
   k_root_frame<<<(S.nseg + 127) / 128, 128, 0, s>>>(S);
+  mark(s, "build.bounds");
   cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * 8 * 256, s);
   k_morton<<<grid_for(n), kBlock, 0, s>>>(S, sort.keys[0], sort.hist);
+  mark(s, "build.morton");
   int buf = radix_sort_u64(s, sort, n, nullptr, 0, 64, true, true, S.status);
+  mark(s, "build.sort");
   if (S.nseg > 1) {
     // stable passes on the instance id keep instances in their ranges
     k_seg_keys<<<grid_for(n), kBlock, 0, s>>>(S, sort.vals[buf], sort.keys[buf]);
@@ -518,6 +521,7 @@ void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
     buf = radix_sort_u64(s, sort, n, nullptr, 0, segBits, false, false, S.status);
   }
   k_gather<<<grid_for(n), kBlock, 0, s>>>(S, sort.vals[buf]);
+  mark(s, "build.gather");
   // swap the double-buffered state: the host mirrors this swap
   DevState T = S;
   T.pv = S.pv2;
@@ -533,16 +537,22 @@ void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
                      scan, S.status);
   k_split_emit<<<grid_for(n), kBlock, 0, s>>>(S, sort.keys[0], sort.vals[0]);
   const int depthBits = S.nseg <= 4 ? 8 : (S.nseg <= 1024 ? 16 : 24);
+  mark(s, "tree.split_emit");
   const int eb = radix_sort_u64(s, sort, 2 * n + 64, &S.counters[3], 0,
                                 depthBits, false, false, S.status);
+  mark(s, "tree.entry_sort");
   cudaMemsetAsync(S.groupStart, 0, sizeof(uint32_t) * S.nseg * kLevelSlots, s);
   cudaMemsetAsync(S.groupEnd, 0, sizeof(uint32_t) * S.nseg * kLevelSlots, s);
   k_groups<<<grid_for(2 * n), kBlock, 0, s>>>(S, sort.keys[eb]);
   k_levels<<<1, 1024, 0, s>>>(S);
+  mark(s, "tree.levels");
   k_split_nodes<<<grid_for(n / 4 + 64), kBlock, 0, s>>>(S, sort.keys[eb],
                                                         sort.vals[eb]);
+  mark(s, "tree.split_nodes");
   k_upward<<<grid_for(n), kBlock, 0, s>>>(S);
+  mark(s, "tree.upward");
   k_preorder<<<grid_for(n), kBlock, 0, s>>>(S);
+  mark(s, "tree.preorder");
 }
 
 } // namespace nbx

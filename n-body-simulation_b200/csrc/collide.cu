@@ -388,6 +388,25 @@ __device__ __forceinline__ uint32_t chain_position(const DevState &S,
   return lo;
 }
 
+// Chain position of each as-later pair (L, E): where L sits in E's sorted
+// partner list.  Computed in bulk so the resolution does not search.
+__global__ void __launch_bounds__(kBlock) k_twins(DevState S) {
+  for (uint32_t L = blockIdx.x * blockDim.x + threadIdx.x; L < S.n;
+       L += gridDim.x * blockDim.x) {
+    const uint32_t nl = S.nLater[L];
+    if (!nl) continue;
+    const uint32_t pl = S.pstart[L];
+    const float key = S.box[L].x;
+    for (uint32_t k = 0; k < nl; ++k)
+      S.twin[pl + k] = chain_position(S, S.plist[pl + k], L, key);
+  }
+}
+
+// Ordered resolution.  A warp claims 32 consecutive units (before() order)
+// and loops: every lane whose next pair is ready (body E has completed the
+// chain entries before this pair) resolves it; lanes that are not ready
+// simply try again next round.  No lane ever spins alone, so a lane whose
+// predecessor belongs to another lane of the same warp cannot starve it.
 __global__ void __launch_bounds__(kBlock)
     k_resolve(DevState S, const uint32_t *__restrict__ units) {
   const uint32_t numUnits = S.counters[1];
@@ -399,38 +418,48 @@ __global__ void __launch_bounds__(kBlock)
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= numUnits) break;
     const uint32_t u = base + lane;
-    if (u < numUnits) {
-      const uint32_t L = units[u];
+    bool active = u < numUnits;
+    uint32_t L = 0, nl = 0, pl = 0, k = 0, E = 0, m = 0;
+    float2 mrL = make_float2(0.0f, 0.0f);
+    float4 sL = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (active) {
+      L = units[u];
       S.unitOrder[u] = L; // kept for introspection of the pair order
-      const uint32_t nl = S.nLater[L];
-      const uint32_t pl = S.pstart[L];
-      const float lKey = S.box[L].x;
-      const float2 mrL = S.mr[L];
-      float4 sL = S.pv[L];
-      bool ok = true;
-      for (uint32_t k = 0; k < nl && ok; ++k) {
-        const uint32_t E = S.plist[pl + k];
-        const uint32_t m = chain_position(S, E, L, lKey);
-        uint32_t spins = 0;
-        while (ld_acquire_u32(&S.prog[E]) != m) {
-          if (++spins > kSpinLimit) {
-            atomicOr(S.status, kStatusSpinLimit);
-            ok = false;
-            break;
-          }
-          __nanosleep(128);
-        }
-        if (!ok) break;
+      nl = S.nLater[L];
+      pl = S.pstart[L];
+      mrL = S.mr[L];
+      sL = S.pv[L];
+      E = S.plist[pl];
+      m = S.twin[pl];
+    }
+    uint32_t idle = 0;
+    while (__any_sync(0xffffffffu, active)) {
+      bool progressed = false;
+      if (active && ld_acquire_u32(&S.prog[E]) == m) {
         const float2 mrE = S.mr[E];
         float4 sE = __ldcg(&S.pv[E]);
         resolve_pair(sL, mrL.x, mrL.y, sE, mrE.x, mrE.y);
         __stcg(&S.pv[E], sE);
-        __threadfence();
         st_release_u32(&S.prog[E], m + 1);
+        progressed = true;
+        if (++k == nl) {
+          __stcg(&S.pv[L], sL);
+          st_release_u32(&S.prog[L], nl);
+          active = false;
+        } else {
+          E = S.plist[pl + k];
+          m = S.twin[pl + k];
+        }
       }
-      __stcg(&S.pv[L], sL);
-      __threadfence();
-      st_release_u32(&S.prog[L], nl);
+      if (__any_sync(0xffffffffu, progressed)) {
+        idle = 0;
+      } else {
+        if (++idle > kSpinLimit) {
+          if (lane == 0) atomicOr(S.status, kStatusSpinLimit);
+          break;
+        }
+        __nanosleep(32);
+      }
     }
   }
 }
@@ -534,22 +563,28 @@ void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
   exclusive_scan_u32(s, S.largeCount, S.largeStartA, S.nseg, nullptr, nullptr,
                      scan, S.status);
   k_fill_grid<<<grid_for(n), kBlock, 0, s>>>(S);
+  mark(s, "collide.grid");
   // partners: count, scan, fill + sort
   k_partners<false><<<grid_for(n), kBlock, 0, s>>>(S);
   exclusive_scan_u32(s, S.deg, S.pstart, n, nullptr, &S.counters[0], scan,
                      S.status);
+  mark(s, "collide.count");
   k_partners<true><<<grid_for(n), kBlock, 0, s>>>(S);
   k_sort_large<<<64, kBlock, 0, s>>>(S);
+  mark(s, "collide.fill");
   // units in before() order
   exclusive_scan_u32(s, S.unitFlag, S.unitPos, n, nullptr, &S.counters[1],
                      scan, S.status);
   k_units<<<grid_for(n), kBlock, 0, s>>>(S, sort.keys[0], sort.vals[0]);
   const int buf = radix_sort_u64(s, sort, n, &S.counters[1], 0, 32, false,
                                  false, S.status);
+  mark(s, "collide.units");
   // ordered resolution
   cudaMemsetAsync(S.prog, 0, sizeof(uint32_t) * n, s);
   cudaMemsetAsync(&S.counters[2], 0, sizeof(uint32_t), s);
+  k_twins<<<grid_for(n), kBlock, 0, s>>>(S);
   k_resolve<<<148 * 8, kBlock, 0, s>>>(S, sort.vals[buf]);
+  mark(s, "collide.resolve");
 }
 
 void launch_bounds(cudaStream_t s, const DevState &S) {

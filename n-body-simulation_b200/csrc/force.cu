@@ -74,9 +74,12 @@ __device__ __forceinline__ float sq_dist(float dx, float dy) {
   return fmaf(dx, dx, dy * dy);
 }
 
-template <bool kExact>
+// kCount: instead of writing accelerations, add the walk's far (accepted,
+// mass > 0), near (leaf body terms) and visited-node counts to counts[0..2].
+template <bool kExact, bool kCount = false>
 __global__ void __launch_bounds__(kForceBlock)
-    k_forces(DevState S, float tSq, float eSq) {
+    k_forces(DevState S, float tSq, float eSq,
+             unsigned long long *counts = nullptr) {
   __shared__ float4 sA[kWarps][32];
   __shared__ int4 sB[kWarps][32];
   __shared__ float4 sBody[kWarps][32];
@@ -101,11 +104,15 @@ __global__ void __launch_bounds__(kForceBlock)
       }
     }
     float ax = 0.0f, ay = 0.0f;
-    uint32_t tileBase = kDone;
+    uint32_t nFar = 0, nNear = 0, nVisit = 0, nIter = 0, nTile = 0;
+    // k - tileBase >= 32 (unsigned) forces the first tile load
+    uint32_t tileBase = 0xffffffe0u;
     for (;;) {
       const uint32_t k = __reduce_min_sync(0xffffffffu, cur);
       if (k == kDone) break;
-      if (tileBase == kDone || k < tileBase || k >= tileBase + 32) {
+      if (kCount) ++nIter;
+      if (k - tileBase >= 32u) {
+        if (kCount) ++nTile;
         tileBase = k;
         const uint32_t g = k + lane;
         if (g < totalNodes) {
@@ -116,21 +123,25 @@ __global__ void __launch_bounds__(kForceBlock)
       }
       const float4 A = sA[w][k - tileBase];
       const int4 B = sB[w][k - tileBase];
-      bool openLeaf = false;
-      if (cur == k) {
-        const float dx = kExact ? __fsub_rn(A.x, x) : A.x - x;
-        const float dy = kExact ? __fsub_rn(A.y, y) : A.y - y;
-        const float dSq = sq_dist<kExact>(dx, dy);
-        const float far = kExact ? __fmul_rn(dSq, tSq) : dSq * tSq;
-        if (A.w < far) {
-          if (A.z > 0.0f) add_term<kExact>(dx, dy, dSq, A.z, eSq, ax, ay);
-          cur = (uint32_t)B.x > k ? (uint32_t)B.x : kDone;
-        } else if (B.w) {
-          openLeaf = true;
-        } else {
-          cur = k + 1;
-        }
+      const uint32_t nxt = (uint32_t)B.x > k ? (uint32_t)B.x : kDone;
+      // every lane evaluates the node; only the lanes waiting at it use it
+      const bool at = cur == k;
+      const float dx = kExact ? __fsub_rn(A.x, x) : A.x - x;
+      const float dy = kExact ? __fsub_rn(A.y, y) : A.y - y;
+      const float dSq = sq_dist<kExact>(dx, dy);
+      const float far = kExact ? __fmul_rn(dSq, tSq) : dSq * tSq;
+      const bool accept = at && A.w < far;
+      const bool openLeaf = at && !accept && B.w != 0;
+      {
+        float tx = ax, ty = ay;
+        add_term<kExact>(dx, dy, dSq, A.z, eSq, tx, ty);
+        const bool use = accept && A.z > 0.0f;
+        ax = use ? tx : ax;
+        ay = use ? ty : ay;
+        if (kCount) nFar += use ? 1u : 0u;
       }
+      if (kCount) nVisit += at ? 1u : 0u;
+      cur = accept ? nxt : ((at && !openLeaf) ? k + 1 : cur);
       const uint32_t leafLanes = __ballot_sync(0xffffffffu, openLeaf);
       if (leafLanes) {
         const uint32_t b0 = (uint32_t)B.y, b1 = (uint32_t)B.z;
@@ -140,25 +151,93 @@ __global__ void __launch_bounds__(kForceBlock)
           __syncwarp();
           if ((uint32_t)lane < cnt) sBody[w][lane] = S.xym[base + lane];
           __syncwarp();
-          if (openLeaf) {
-            for (uint32_t j = 0; j < cnt; ++j) {
-              const float4 q = sBody[w][j];
-              const float ex = kExact ? __fsub_rn(q.x, x) : q.x - x;
-              const float ey = kExact ? __fsub_rn(q.y, y) : q.y - y;
-              add_term<kExact>(ex, ey, sq_dist<kExact>(ex, ey), q.z, eSq, ax,
-                               ay);
-            }
+#pragma unroll 4
+          for (uint32_t j = 0; j < cnt; ++j) {
+            const float4 q = sBody[w][j];
+            const float ex = kExact ? __fsub_rn(q.x, x) : q.x - x;
+            const float ey = kExact ? __fsub_rn(q.y, y) : q.y - y;
+            float tx = ax, ty = ay;
+            add_term<kExact>(ex, ey, sq_dist<kExact>(ex, ey), q.z, eSq, tx, ty);
+            ax = openLeaf ? tx : ax;
+            ay = openLeaf ? ty : ay;
           }
         }
-        if (openLeaf) cur = (uint32_t)B.x > k ? (uint32_t)B.x : kDone;
+        if (kCount && openLeaf) nNear += bEnd > b0 ? bEnd - b0 : 0u;
+        cur = openLeaf ? nxt : cur;
       }
-      if (cur != kDone && cur >= endNode) cur = kDone;
+      cur = cur >= endNode ? kDone : cur;
     }
-    if (valid) S.acc[i] = make_float2(ax, ay);
+    if (kCount) {
+      unsigned long long f = nFar, nn = nNear, v = nVisit;
+      for (int o = 16; o > 0; o >>= 1) {
+        f += __shfl_xor_sync(0xffffffffu, f, o);
+        nn += __shfl_xor_sync(0xffffffffu, nn, o);
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+      }
+      if (lane == 0) {
+        atomicAdd(&counts[0], f);
+        atomicAdd(&counts[1], nn);
+        atomicAdd(&counts[2], v);
+        atomicAdd(&counts[3], (unsigned long long)nIter);
+        atomicAdd(&counts[4], (unsigned long long)nTile);
+      }
+    } else if (valid) {
+      S.acc[i] = make_float2(ax, ay);
+    }
   }
 }
 
+// FMA throughput probe: 8 independent chains per thread.
+__global__ void k_fma_probe(float *out, int iters) {
+  float a[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) a[j] = threadIdx.x * 1e-7f + j;
+  const float b = 0.999999f, c = 1e-7f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = fmaf(a[j], b, c);
+  }
+  float s = 0.0f;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s += a[j];
+  if (s == 12345.0f) out[0] = s; // keeps the chains live
+}
+
 } // namespace
+
+void launch_interaction_count(cudaStream_t s, const DevState &S,
+                              unsigned long long *counts) {
+  uint32_t warps = (S.n + 31) / 32;
+  uint32_t b = (warps + kWarps - 1) / kWarps;
+  cudaMemsetAsync(counts, 0, 5 * sizeof(unsigned long long), s);
+  k_forces<false, true><<<b ? b : 1, kForceBlock, 0, s>>>(S, S.tSq, S.eSq, counts);
+}
+
+// FP32 FMA peak of the device in TFLOP/s (2 flops per FMA), timed with
+// CUDA events around one large probe launch.
+double fp32_fma_peak_tflops(cudaStream_t s) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  float *out = nullptr;
+  if (cudaMalloc(&out, 4) != cudaSuccess) return 0.0;
+  const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+  k_fma_probe<<<blocks, threads, 0, s>>>(out, 64); // warm-up
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, s);
+  k_fma_probe<<<blocks, threads, 0, s>>>(out, iters);
+  cudaEventRecord(e1, s);
+  cudaEventSynchronize(e1);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  const double flops = 2.0 * 8.0 * (double)iters * blocks * threads;
+  return ms > 0 ? flops / (ms * 1e-3) / 1e12 : 0.0;
+}
 
 void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks) {
   if (blocks <= 0) {

@@ -53,6 +53,22 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return m;
 }
 
+// Optional phase markers: when a profiling step is running on this thread
+// (nbx_profile_step), launch sequences record an event after each stage.
+struct PhaseMarks {
+  static constexpr int kMax = 48;
+  cudaEvent_t ev[kMax];
+  const char *label[kMax];
+  int count = 0;
+};
+extern thread_local PhaseMarks *g_marks;
+inline void mark(cudaStream_t s, const char *label) {
+  if (g_marks && g_marks->count < PhaseMarks::kMax) {
+    cudaEventRecord(g_marks->ev[g_marks->count], s);
+    g_marks->label[g_marks->count++] = label;
+  }
+}
+
 // Grid-stride helpers sized from a device-side count.
 __device__ __forceinline__ uint32_t load_count(const uint32_t *d_n, uint32_t n) {
   return d_n ? *d_n : n;

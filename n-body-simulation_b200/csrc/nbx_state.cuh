@@ -67,6 +67,7 @@ struct DevState {
   uint32_t *pstart;      // CSR start per body
   uint32_t *plist;       // partner indices
   uint32_t *plistTmp;    // scratch copy used to sort large bodies' lists
+  uint32_t *twin;        // per as-later entry: position in the partner's list
   uint32_t *fillLarge;   // fill counters of large bodies
   uint32_t *nLater;      // partners that sort before the body
   uint32_t *unitFlag;    // nLater > 0

@@ -32,6 +32,8 @@ EXPORTS = (
     "nbx_get_pairs", "nbx_direct_fp64", "nbx_force_error_fp64",
     "nbx_energy_momentum_fp64", "nbx_status_bits", "nbx_last_error",
     "nbx_uniform_disc", "nbx_two_discs", "nbx_cold_square", "nbx_version",
+    "nbx_get_stream", "nbx_step_kernel_count", "nbx_interaction_count",
+    "nbx_fp32_peak_tflops", "nbx_profile_step",
 )
 
 PHASE = {"iterate": 0, "collide": 1, "build": 2, "forces": 3, "attract": 4,
@@ -46,7 +48,7 @@ class Params(C.Structure):
                 ("leaf_capacity", C.c_int32), ("collisions", C.c_int32),
                 ("exact_math", C.c_int32), ("use_mlp", C.c_int32),
                 ("node_factor", C.c_float), ("pair_factor", C.c_float),
-                ("force_blocks", C.c_int32)]
+                ("force_blocks", C.c_int32), ("device", C.c_int32)]
 
 
 class NbxError(RuntimeError):
@@ -98,6 +100,11 @@ def lib() -> C.CDLL:
         "nbx_two_discs": [C.c_uint32, C.c_uint32, C.c_float, bodyp],
         "nbx_cold_square": [C.c_uint32, C.c_uint32, bodyp],
         "nbx_version": [],
+        "nbx_get_stream": [vp, C.POINTER(vp)],
+        "nbx_step_kernel_count": [vp, C.POINTER(C.c_uint32)],
+        "nbx_interaction_count": [vp, f64p],
+        "nbx_fp32_peak_tflops": [C.POINTER(C.c_double)],
+        "nbx_profile_step": [vp, C.c_uint32, vp, vp, C.POINTER(C.c_uint32)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -115,6 +122,12 @@ def default_params(**kw) -> Params:
     for k, v in kw.items():
         setattr(p, k, v)
     return p
+
+
+def fp32_peak_tflops() -> float:
+    v = C.c_double()
+    _check(None, lib().nbx_fp32_peak_tflops(C.byref(v)))
+    return v.value
 
 
 def uniform_disc(n: int, seed: int = 0) -> np.ndarray:
@@ -266,6 +279,34 @@ class Handle:
         out = np.zeros(5, np.float64)
         self._c(lib().nbx_energy_momentum_fp64(self.h, out))
         return out
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._c(lib().nbx_get_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def step_kernels(self) -> int:
+        k = C.c_uint32()
+        self._c(lib().nbx_step_kernel_count(self.h, C.byref(k)))
+        return k.value
+
+    def interactions(self):
+        out = np.zeros(5, np.float64)
+        self._c(lib().nbx_interaction_count(self.h, out))
+        return {"far": out[0], "near": out[1], "visits": out[2],
+                "warp_iters": out[3], "tile_loads": out[4]}
+
+    def profile_step(self) -> dict:
+        """One eager step; milliseconds per stage."""
+        m = 48
+        labels = C.create_string_buffer(32 * m)
+        ms = np.zeros(m, np.float32)
+        cnt = C.c_uint32()
+        self._c(lib().nbx_profile_step(self.h, m, labels, ms.ctypes.data,
+                                       C.byref(cnt)))
+        raw = labels.raw
+        return {raw[32 * k: 32 * k + 32].split(b"\0")[0].decode(): float(ms[k])
+                for k in range(cnt.value)}
 
     def status_bits(self) -> int:
         b = C.c_uint32()

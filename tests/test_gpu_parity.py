@@ -1,0 +1,303 @@
+"""GPU parity: the sm_100a path (through the C ABI) against the CPU oracle
+on the same inputs.  Integer/index outputs are bit-exact; with
+exact_math=1 the float outputs are bit-exact too; the default (contracted)
+arithmetic is held to the reference's own bars (CheckCuda.cu)."""
+import numpy as np
+import pytest
+
+from conftest import bits, rel_err, same_bits
+
+pytestmark = pytest.mark.gpu
+
+
+def with_central_contacts(state, count=8):
+    """Small bodies placed overlapping the heaviest body at spread angles and
+    varied velocities (withCentralContacts, CheckCuda.cu:198-227)."""
+    s = state.copy()
+    c = int(np.argmax(s["radius"]))
+    n = len(s)
+    for k in range(count):
+        i = (k + 1) * n // (count + 1)
+        if i == c:
+            i += 1
+        ang = np.float32(6.2831853 * k / count)
+        d = np.array([np.cos(ang), np.sin(ang)], np.float32)
+        depth = np.float32(0.2 + 0.1 * k)
+        pos = np.array([s["px"][c], s["py"][c]], np.float32) + d * (
+            s["radius"][c] + s["radius"][i] - depth)
+        t = np.array([-d[1], d[0]], np.float32)
+        v = [d * -5.0, d * 3.0, t * 4.0][k % 3]
+        s["px"][i], s["py"][i] = pos
+        s["vx"][i] = s["vx"][c] + v[0]
+        s["vy"][i] = s["vy"][c] + v[1]
+    return s
+
+
+def gpu_build(nbx, bodies, **kw):
+    sim = nbx.Simulation(bodies, **kw)
+    sim.phase("build")
+    return sim
+
+
+STATES = {}
+
+
+def state(nbx, oracle, name):
+    if name in STATES:
+        return STATES[name]
+    if name == "disc10k":
+        s = nbx.uniform_disc(10000)
+    elif name == "disc200k":
+        s = nbx.uniform_disc(200000)
+    elif name == "two_discs65k":
+        s = nbx.two_discs(65536, 0, 0.2)
+    elif name == "cold50k":
+        s = nbx.cold_square(50000, 1)
+    elif name == "colliding20k":
+        sim = nbx.Simulation(nbx.uniform_disc(20000))
+        sim.step(300)
+        sim.phase("iterate")
+        s = sim.download()
+        sim.close()
+    elif name == "coincident":
+        s = nbx.uniform_disc(3000)
+        s["px"][100:160] = s["px"][100]  # 60 bodies on one point: depth-32 leaf
+        s["py"][100:160] = s["py"][100]
+    else:
+        raise KeyError(name)
+    STATES[name] = s
+    return s
+
+
+@pytest.mark.parametrize("name", ["disc10k", "disc200k", "two_discs65k",
+                                  "cold50k", "coincident"])
+@pytest.mark.parametrize("leaf", [16, 4])
+def test_morton_perm_tree_bit_exact(nbx, oracle, name, leaf):
+    b = state(nbx, oracle, name)
+    sim = gpu_build(nbx, b, leaf_capacity=leaf)
+    codes, perm = sim.morton()
+    root, ocodes, operm, sb, tree = oracle.morton_build(b, leaf)
+    assert np.array_equal(codes, ocodes)
+    assert np.array_equal(perm, operm)
+    t = sim.tree()
+    assert t["node_count"] == tree.node_count
+    assert t["level_count"] == tree.level_count
+    for k, v in tree.trimmed().items():
+        assert same_bits(t[k], v), k
+    # the device state is permuted into Morton order like the reference's
+    assert np.array_equal(sim.download()["id"], sb["id"])
+    sim.close()
+
+
+@pytest.mark.parametrize("name", ["disc10k", "disc200k", "colliding20k", "cold50k"])
+@pytest.mark.parametrize("theta", [1.0, 0.5])
+def test_forces(nbx, oracle, name, theta):
+    b = state(nbx, oracle, name)
+    _, _, _, sb, tree = oracle.morton_build(b)
+    ox, oy = oracle.tree_forces(sb["px"], sb["py"], sb["mass"], tree, theta, 1.0)
+    sim = nbx.Simulation(b, theta=theta, exact_math=1)
+    sim.phase("attract")
+    g = sim.download()
+    # exact arithmetic: bit-identical to the reference traversal
+    assert same_bits(g["ax"], ox) and same_bits(g["ay"], oy)
+    sim.set_params(exact_math=0)
+    sim.phase("forces")
+    g = sim.download()
+    e = rel_err(g["ax"], g["ay"], ox, oy)
+    assert np.percentile(e, 99) < 1e-5 and e.max() < 1e-4, (np.percentile(e, 99), e.max())
+    sim.close()
+
+
+@pytest.mark.parametrize("name", ["disc10k", "colliding20k"])
+def test_forces_vs_partition_quadtree(nbx, oracle, name):
+    """Against QuadTree.cpp's own tree (partition build): the bar of
+    CheckCuda.cu:609-614 (median < 1e-5, p99 < 1e-4)."""
+    b = state(nbx, oracle, name)
+    q = np.sort(oracle.quadtree_forces(b, 1.0, 1.0), order="id")
+    sim = nbx.Simulation(b)
+    sim.phase("attract")
+    g = np.sort(sim.download(), order="id")
+    e = rel_err(g["ax"], g["ay"], q["ax"], q["ay"])
+    assert np.median(e) < 1e-5 and np.percentile(e, 99) < 1e-4
+    sim.close()
+
+
+def collide_cases(nbx, oracle, golden):
+    yield "golden", golden["collide_in"]
+    c20 = state(nbx, oracle, "colliding20k")
+    yield "colliding20k", c20
+    yield "central8", with_central_contacts(c20, 8)
+    big = nbx.uniform_disc(200000)
+    yield "central8_200k", with_central_contacts(oracle.integrate(big, 0.05), 8)
+    cold = nbx.cold_square(20000, 2)
+    cold["px"] *= np.float32(0.35)  # compressed: most boxes overlap neighbours
+    cold["py"] *= np.float32(0.35)
+    yield "cold_dense", cold
+
+
+def test_collisions_bit_exact(nbx, oracle, golden):
+    seen_large = 0
+    for label, st in collide_cases(nbx, oracle, golden):
+        sim = nbx.Simulation(st)
+        sim.phase("collide")
+        gl, ge = sim.pairs()
+        ol, oe = oracle.collision_pairs(st)
+        assert len(ol) > 0, label
+        assert np.array_equal(gl, ol) and np.array_equal(ge, oe), label
+        out = sim.download()
+        ref, _ = oracle.collide(st)
+        assert same_bits(out, ref), (label, int((out != ref).sum()))
+        heavy = int(np.argmax(st["radius"]))
+        seen_large += int(((gl == heavy) | (ge == heavy)).sum())
+        sim.close()
+    assert seen_large > 0  # the large-body path saw real contacts
+
+
+def test_collide_then_reference_bodies(nbx, golden):
+    """Against the reference's own collide() output (fixture)."""
+    sim = nbx.Simulation(golden["collide_in"])
+    sim.phase("collide")
+    assert same_bits(sim.download(), golden["collide_out"])
+    sim.close()
+
+
+@pytest.mark.parametrize("theta", [1.0, 0.5])
+def test_ten_step_trajectories(nbx, oracle, golden, theta):
+    b = nbx.uniform_disc(20000)
+    o = oracle.step(b, steps=10, theta=theta)
+    sim = nbx.Simulation(b, theta=theta, exact_math=1)
+    sim.step(10)
+    sim.sync()
+    assert same_bits(sim.download(), o)  # whole state, bit for bit
+    sim.close()
+    sim = nbx.Simulation(b, theta=theta)
+    sim.step(10)
+    sim.sync()
+    g = np.sort(sim.download(), order="id")
+    r = np.sort(o, order="id")
+    e = rel_err(g["px"], g["py"], r["px"], r["py"])
+    assert e.max() < 1e-3 and np.median(e) < 1e-5, (e.max(), np.median(e))
+    sim.close()
+    # against the reference's own Simulation::step (partition tree)
+    sim = nbx.Simulation(golden["sim_in"], theta=theta)
+    sim.step(10)
+    g = sim.download(id_order=True)
+    r = np.sort(golden[f"sim10_t{theta}"], order="id")
+    e = rel_err(g["px"], g["py"], r["px"], r["py"])
+    assert e.max() < 1e-3 and np.median(e) < 1e-4, (e.max(), np.median(e))
+    sim.close()
+
+
+def test_deterministic(nbx):
+    b = nbx.uniform_disc(20000)
+    outs = []
+    for _ in range(2):
+        sim = nbx.Simulation(b)
+        sim.step(50)
+        outs.append(sim.download())
+        sim.close()
+    assert same_bits(outs[0], outs[1])
+
+
+def test_tree_invariants_1m(nbx):
+    """Size-independent properties at the headline size (1,048,576 bodies)."""
+    b = nbx.two_discs(1 << 20, 0, 0.2)
+    sim = nbx.Simulation(b, theta=0.5)
+    sim.step(3)
+    sim.phase("build")
+    t = sim.tree()
+    s = sim.download()
+    n = len(b)
+    assert np.array_equal(np.sort(s["id"]), np.arange(n))
+    assert abs(float(t["mass"][0]) - float(s["mass"].astype(np.float64).sum())) <= 1e-5 * s["mass"].sum()
+    leaf = t["children"] == 0
+    st, en = t["start"][leaf], t["end"][leaf]
+    order = np.lexsort((en, st))  # empty leaves (s, s) sort before (s, e)
+    st, en = st[order], en[order]
+    assert st[0] == 0 and en[-1] == n and np.array_equal(st[1:], en[:-1])
+    assert (en - st).max() <= 16
+    half = (t["size"][leaf] * 0.5 * 1.0001 + 1e-3)[order]
+    cx, cy = t["centerX"][leaf][order], t["centerY"][leaf][order]
+    owner = np.repeat(np.arange(len(st)), en - st)
+    assert np.all(np.abs(s["px"] - cx[owner]) <= half[owner])
+    assert np.all(np.abs(s["py"] - cy[owner]) <= half[owner])
+    sim.close()
+
+
+def test_fp64_direct_and_energy(nbx, oracle):
+    b = nbx.uniform_disc(20000)
+    sim = nbx.Simulation(b)
+    sim.step(2)
+    s = sim.download()
+    rng = np.random.default_rng(5)
+    tg = rng.choice(len(b), 256, replace=False).astype(np.uint32)
+    gx, gy = sim.direct_fp64(tg)
+    ox, oy = oracle.direct_fp64(s, 1.0, tg)
+    assert np.max(rel_err(gx, gy, ox, oy)) < 1e-12
+    stats, err = sim.force_error(tg)
+    acc = s[tg]
+    e = rel_err(acc["ax"], acc["ay"], ox, oy)
+    assert np.allclose(np.sort(err), np.sort(e), rtol=1e-6, atol=1e-12)
+    em = sim.energy_momentum()
+    oem = oracle.energy_momentum(s)
+    assert np.allclose(em, oem, rtol=1e-12, atol=1e-9)
+    sim.close()
+
+
+def test_id_order_download(nbx):
+    b = nbx.uniform_disc(5000)
+    sim = nbx.Simulation(b)
+    sim.step(3)
+    a = sim.download()
+    o = sim.download(id_order=True)
+    assert np.array_equal(o["id"], np.arange(5000))
+    assert same_bits(np.sort(a, order="id"), o)
+    sim.close()
+
+
+@pytest.mark.parametrize("n", [1, 2, 16, 17, 33])
+def test_small_sizes(nbx, oracle, n):
+    b = nbx.uniform_disc(n)
+    sim = nbx.Simulation(b, exact_math=1)
+    sim.step(3)
+    sim.sync()
+    assert same_bits(sim.download(), oracle.step(b, steps=3))
+    sim.close()
+
+
+def test_empty_instance(nbx):
+    sim = nbx.Simulation(np.zeros(0, nbx.BODY_DTYPE))
+    sim.step(2)
+    sim.sync()
+    assert len(sim.download()) == 0
+    sim.close()
+
+
+def test_nonfinite_reported(nbx):
+    b = nbx.uniform_disc(1000)
+    b["px"][10] = np.nan
+    sim = nbx.Simulation(b)
+    sim.step(1)
+    with pytest.raises(nbx.NbxError) as e:
+        sim.sync()
+    assert e.value.code == 4
+    sim.close()
+
+
+def test_capacity_errors_reported(nbx, oracle):
+    b = nbx.uniform_disc(20000)
+    sim = nbx.Simulation(b, node_factor=0.01)
+    sim.step(1)
+    with pytest.raises(nbx.NbxError) as e:
+        sim.sync()
+    assert e.value.code == 3
+    sim.close()
+    cold = nbx.cold_square(20000, 2)
+    cold["px"] *= np.float32(0.3)
+    cold["py"] *= np.float32(0.3)
+    sim = nbx.Simulation(cold, pair_factor=0.01)
+    sim.phase("iterate")  # no pending error yet
+    with pytest.raises(nbx.NbxError) as e:
+        sim.phase("collide")
+    assert e.value.code == 3
+    sim.close()

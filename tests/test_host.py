@@ -1,0 +1,77 @@
+"""Host-side product code: the C ABI library loads and exports every entry
+point of include/nbx.h; the generators reproduce the reference's initial
+conditions bit for bit.  No GPU needed (no compute calls are made)."""
+import hashlib
+import os
+import re
+
+import numpy as np
+
+from conftest import ROOT, same_bits
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "nbx.h")).read()
+    return sorted(set(re.findall(r"\b(nbx_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_symbols_exported(nbx):
+    lib = nbx.lib()
+    names = declared_symbols()
+    assert len(names) >= 20
+    missing = [s for s in names if not hasattr(lib, s)]
+    assert not missing, missing
+    assert set(names) >= set(nbx.EXPORTS)
+
+
+def test_uniform_disc_matches_reference(nbx, golden):
+    assert same_bits(nbx.uniform_disc(4096), golden["disc4096"])
+    assert same_bits(nbx.uniform_disc(4096, 7), golden["disc4096_seed7"])
+    for n in (10000, 1 << 19):
+        h = hashlib.sha256(nbx.uniform_disc(n).tobytes()).digest()
+        assert h == golden[f"disc{n}_sha256"].tobytes(), n
+
+
+def test_params_default_are_reference_defaults(nbx):
+    p = nbx.default_params()
+    assert (p.dt, p.theta, p.epsilon, p.leaf_capacity, p.collisions) == (
+        np.float32(0.05), 1.0, 1.0, 16, 1)
+
+
+def test_two_discs_layout(nbx):
+    n = 2048
+    b = nbx.two_discs(n, 0, 0.2)
+    assert np.array_equal(b["id"], np.arange(n))
+    left, right = b[: n // 2], b[n // 2:]
+    assert left["px"].mean() < 0 < right["px"].mean()
+    assert (left["mass"] == 1e6).sum() == 1 and (right["mass"] == 1e6).sum() == 1
+    # opposite spins: angular momentum about each centre has opposite sign
+    def lz(d):
+        x = d["px"] - d["px"][d["mass"] > 1e5][0]
+        y = d["py"] - d["py"][d["mass"] > 1e5][0]
+        vy = d["vy"] - d["vy"][d["mass"] > 1e5][0]
+        vx = d["vx"] - d["vx"][d["mass"] > 1e5][0]
+        return float((d["mass"] * (x * vy - y * vx)).sum())
+    assert lz(left) * lz(right) < 0
+
+
+def test_cold_square(nbx):
+    b = nbx.cold_square(1000, 3)
+    h = 3 * np.sqrt(1000)
+    assert np.all(np.abs(b["px"]) <= h) and np.all(np.abs(b["py"]) <= h)
+    assert np.all(b["vx"] == 0) and np.all(b["radius"] == 1) and np.all(b["mass"] == 1)
+
+
+def test_create_without_device_reports_error(nbx):
+    """On a machine without a GPU nbx_create returns an error code instead
+    of exiting (the reference's CUDA_CHECK aborts the process)."""
+    import subprocess, sys
+    code = ("import sys; sys.path.insert(0, %r); import nbx\n"
+            "try:\n    nbx.Handle([16])\n    print('created')\n"
+            "except nbx.NbxError as e:\n    print('error', e.code)\n"
+            % os.path.join(ROOT, "n-body-simulation_b200"))
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True,
+                         text=True, env=env, timeout=120)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.startswith("error"), out.stdout
