@@ -60,12 +60,17 @@ typedef struct nbx_params {
                              writes it (no FMA contraction, IEEE reciprocal),
                              bit-identical to the CPU traversal on the same
                              tree; 0: contracted, hardware reciprocal */
-  int32_t use_mlp;        /* 1: learned far-field correction (nbx_mlp_*) */
+  int32_t use_mlp;        /* far-field correction of accepted cells with
+                             size/distance >= mlp_band: 0 none (the
+                             reference), 1 learned MLP (nbx_mlp_*), 2 the
+                             analytic quadrupole term (control) */
   float node_factor;      /* node capacity per body (default 8, the
                              reference bound 8n+8, CudaQuadTree.cu:270-273) */
   float pair_factor;      /* collision partner slots per body (default 32) */
   int32_t force_blocks;   /* 0 = auto; else blocks of the force launch */
   int32_t device;         /* CUDA device ordinal; -1 = the current device */
+  float mlp_band;         /* learned correction on accepted cells with
+                             size/distance >= mlp_band (default 0.5) */
 } nbx_params;
 
 typedef struct nbx_handle nbx_handle;
@@ -198,6 +203,47 @@ int nbx_fp32_peak_tflops(double *tflops);
 /* Device status bits (cleared on read) and the last error message. */
 int nbx_status_bits(nbx_handle *h, uint32_t *bits);
 const char *nbx_last_error(const nbx_handle *h);
+
+/* --- learned far-field correction (no counterpart in the reference) ---
+ * A 9 -> 32 -> 32 -> 2 SiLU MLP with BF16 weights and FP32 accumulation
+ * corrects the monopole of accepted cells with size/distance >= mlp_band
+ * when params.use_mlp = 1.  Parameters are 1442 FP32 values:
+ * W1[32][9], b1[32], W2[32][32], b2[32], W3[2][32], b3[2].  A training row
+ * is 12 floats: 9 features, 2 targets, weight. */
+#define NBX_MLP_PARAMS 1442
+#define NBX_MLP_ROW 12
+
+int nbx_mlp_set_params(nbx_handle *h, const float *params, uint32_t n);
+int nbx_mlp_get_params(nbx_handle *h, float *params, uint32_t n);
+
+/* Xavier-uniform weights, zero biases, from mt19937(seed). */
+int nbx_mlp_init(nbx_handle *h, uint32_t seed);
+
+/* Walks the last tree from the bodies at the given current indices with
+ * MAC theta; every accepted cell with size/distance >= band yields a row
+ * whose targets come from an FP64 direct sum over the cell's bodies.
+ * Writes at most max_rows rows; *n_rows receives the number written. */
+int nbx_mlp_harvest(nbx_handle *h, const uint32_t *targets, uint32_t n_targets,
+                    float theta, float band, float *rows, uint32_t max_rows,
+                    uint32_t *n_rows);
+
+/* Adam on the mean weighted squared error of the rows, minibatches of
+ * `batch` rows in an order shuffled per epoch by mt19937(seed);
+ * epoch_loss (epochs entries, may be NULL) receives the mean loss. */
+int nbx_mlp_train(nbx_handle *h, const float *rows, uint32_t n_rows,
+                  uint32_t epochs, uint32_t batch, float lr, uint32_t seed,
+                  float *epoch_loss);
+
+/* Gradient (1442 floats) and loss of the mean weighted squared error over
+ * all rows, with the training kernels (for gradient checks). */
+int nbx_mlp_gradient(nbx_handle *h, const float *rows, uint32_t n_rows,
+                     float *grad, float *loss);
+
+/* Network outputs (2 per row) for n feature rows of 9 floats, with the
+ * training kernels (tensor_cores = 0) or the tensor-core inference path
+ * of the traversal (tensor_cores = 1). */
+int nbx_mlp_eval(nbx_handle *h, const float *features, uint32_t n, float *out,
+                 int tensor_cores);
 
 /* --- host-side scenario generators (product host code) --- */
 

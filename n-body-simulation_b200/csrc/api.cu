@@ -1,6 +1,7 @@
 // api.cu -- the C ABI (include/nbx.h): handles, device memory, step
 // sequencing and graph capture, introspection for parity checks.
 #include "nbx.h"
+#include "mlp.cuh"
 #include "nbx_state.cuh"
 
 #include <algorithm>
@@ -8,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -19,7 +21,20 @@ void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
 void launch_bounds(cudaStream_t s, const DevState &S);
 void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
                   SortScratch &sort);
-void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks);
+void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
+                   const MlpDev *mlp, float band, int corr);
+void mlp_harvest(cudaStream_t s, const DevState &S, const uint32_t *targets,
+                 uint32_t nt, float theta, float band, float eps, uint2 *items,
+                 uint32_t cap, uint32_t *count, float *rows);
+void mlp_pack(cudaStream_t s, const float *P, MlpDev *W);
+void mlp_gradient(cudaStream_t s, const float *rows, const uint32_t *order,
+                  uint32_t first, uint32_t batch, const float *P, float *partial,
+                  float *lossPart, float *grad, float *loss);
+void mlp_adam(cudaStream_t s, float *P, const float *grad, float *m, float *v,
+              int step, float lr, MlpDev *W);
+void mlp_eval(cudaStream_t s, const float *feat, uint32_t n, const float *P,
+              const MlpDev *W, float *out, bool tensor);
+int mlp_rows_per_block();
 void launch_interaction_count(cudaStream_t s, const DevState &S,
                               unsigned long long *counts);
 double fp32_fma_peak_tflops(cudaStream_t s);
@@ -128,6 +143,12 @@ struct nbx_handle {
   double *dF64 = nullptr;       // small FP64 scratch
   uint32_t *dTargets = nullptr;
   std::string lastError;
+  // learned correction
+  float *mlpP = nullptr, *mlpM = nullptr, *mlpV = nullptr, *mlpGrad = nullptr;
+  MlpDev *mlpW = nullptr;
+  bool mlpLoaded = false;
+  int mlpStep = 0;
+  std::vector<void *> scratch; // grow-on-demand buffers (MLP data)
 
   DevState state() const {
     DevState S = base;
@@ -269,6 +290,12 @@ int allocate(nbx_handle *h) {
   A(sc.tileCounter, 1);
   A(h->dAoS, n);
   A(h->dF64, 16 * 592);
+  A(S.tC, nodes);
+  A(h->mlpP, kMlpParams);
+  A(h->mlpM, kMlpParams);
+  A(h->mlpV, kMlpParams);
+  A(h->mlpGrad, kMlpParams + 1);
+  A(h->mlpW, 1);
 #undef A
   // bounds accumulators start empty
   std::vector<uint32_t> b(4 * ns);
@@ -321,7 +348,9 @@ DevState enqueue_step(nbx_handle *h, cudaStream_t s, DevState S) {
   mark(s, "integrate");
   if (S.collisions) launch_collide(s, S, h->scan, h->sort);
   launch_build(s, S, h->scan, h->sort);
-  launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks);
+  launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
+                h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
+                h->params.use_mlp);
   mark(s, "forces");
   return S;
 }
@@ -385,7 +414,8 @@ int check_status(nbx_handle *h) {
 
 bool valid_params(const nbx_params *p) {
   return p && p->dt == p->dt && p->theta >= 0.0f && p->epsilon >= 0.0f &&
-         p->leaf_capacity >= 1 && p->leaf_capacity <= 64;
+         p->leaf_capacity >= 1 && p->leaf_capacity <= 64 && p->use_mlp >= 0 &&
+         p->use_mlp <= 2;
 }
 
 } // namespace
@@ -408,6 +438,7 @@ int nbx_params_default(nbx_params *p) {
   p->pair_factor = 32.0f;
   p->force_blocks = 0;
   p->device = -1;
+  p->mlp_band = 0.5f;
   return NBX_OK;
 }
 
@@ -454,6 +485,7 @@ int nbx_destroy(nbx_handle *h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   destroy_graphs(h);
   for (void *v : h->allocs) cudaFree(v);
+  for (void *v : h->scratch) cudaFree(v);
   if (h->hPinned) cudaFreeHost(h->hPinned);
   if (h->dPartial) cudaFree(h->dPartial);
   if (h->dTargets) cudaFree(h->dTargets);
@@ -580,6 +612,8 @@ int nbx_step(nbx_handle *h, uint32_t steps) {
   cudaSetDevice(h->device);
   if (!h->uploaded) return fail(h, NBX_ERR_STATE, "no bodies uploaded");
   if (h->n == 0 || steps == 0) return NBX_OK;
+  if (h->params.use_mlp == 1 && !h->mlpLoaded)
+    return fail(h, NBX_ERR_STATE, "use_mlp = 1 without MLP parameters");
   if (!h->graphsValid) {
     int rc = capture_graphs(h);
     if (rc != NBX_OK) return rc;
@@ -625,13 +659,17 @@ int nbx_phase(nbx_handle *h, int phase) {
     break;
   case NBX_PHASE_FORCES:
     if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
-    launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks);
+    launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
+                  h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
+                  h->params.use_mlp);
     break;
   case NBX_PHASE_ATTRACT:
     launch_build(s, S, h->scan, h->sort);
     h->cur ^= 1;
     h->treeValid = true;
-    launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks);
+    launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
+                  h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
+                  h->params.use_mlp);
     break;
   case NBX_PHASE_STEP:
     enqueue_step(h, s, S);
@@ -845,6 +883,196 @@ int nbx_profile_step(nbx_handle *h, uint32_t max_marks, char *labels,
   for (int k = 0; k < PhaseMarks::kMax; ++k) cudaEventDestroy(marks.ev[k]);
   if (e != cudaSuccess) return cuda_fail(h, e, "profile step");
   return check_status(h);
+}
+
+// ---------------------------------------------------------------- MLP
+static int scratch_alloc(nbx_handle *h, void **p, size_t bytes) {
+  NBX_CUDA(h, cudaMalloc(p, std::max<size_t>(bytes, 16)));
+  h->scratch.push_back(*p);
+  return NBX_OK;
+}
+
+static void scratch_free(nbx_handle *h, void *p) {
+  for (auto it = h->scratch.begin(); it != h->scratch.end(); ++it)
+    if (*it == p) {
+      cudaFree(p);
+      h->scratch.erase(it);
+      return;
+    }
+}
+
+int nbx_mlp_set_params(nbx_handle *h, const float *params, uint32_t n) {
+  if (!h || !params || n != (uint32_t)kMlpParams) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  NBX_CUDA(h, cudaMemcpyAsync(h->mlpP, params, 4ull * n, cudaMemcpyHostToDevice, h->stream));
+  NBX_CUDA(h, cudaMemsetAsync(h->mlpM, 0, 4ull * n, h->stream));
+  NBX_CUDA(h, cudaMemsetAsync(h->mlpV, 0, 4ull * n, h->stream));
+  mlp_pack(h->stream, h->mlpP, h->mlpW);
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->mlpLoaded = true;
+  h->mlpStep = 0;
+  destroy_graphs(h);
+  return NBX_OK;
+}
+
+int nbx_mlp_get_params(nbx_handle *h, float *params, uint32_t n) {
+  if (!h || !params || n != (uint32_t)kMlpParams) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  NBX_CUDA(h, cudaMemcpyAsync(params, h->mlpP, 4ull * n, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  return NBX_OK;
+}
+
+int nbx_mlp_init(nbx_handle *h, uint32_t seed) {
+  if (!h) return NBX_ERR_ARG;
+  std::vector<float> P(kMlpParams, 0.0f);
+  std::mt19937 rng(seed);
+  auto fill = [&](int off, int rows, int cols) {
+    const float a = std::sqrt(6.0f / (float)(rows + cols));
+    std::uniform_real_distribution<float> u(-a, a);
+    for (int i = 0; i < rows * cols; ++i) P[off + i] = u(rng);
+  };
+  fill(kOffW1, 32, 9);
+  fill(kOffW2, 32, 32);
+  fill(kOffW3, 2, 32);
+  for (int i = 0; i < 2 * 32; ++i) P[kOffW3 + i] *= 0.1f; // start near zero correction
+  return nbx_mlp_set_params(h, P.data(), kMlpParams);
+}
+
+int nbx_mlp_harvest(nbx_handle *h, const uint32_t *targets, uint32_t nt,
+                    float theta, float band, float *rows, uint32_t maxRows,
+                    uint32_t *nRows) {
+  if (!h || !nRows || (nt && !targets) || (maxRows && !rows)) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
+  for (uint32_t k = 0; k < nt; ++k)
+    if (targets[k] >= h->n) return fail(h, NBX_ERR_ARG, "target index out of range");
+  *nRows = 0;
+  if (nt == 0 || maxRows == 0) return NBX_OK;
+  void *dT = nullptr, *dItems = nullptr, *dRows = nullptr, *dCount = nullptr;
+  int rc = scratch_alloc(h, &dT, 4ull * nt);
+  if (!rc) rc = scratch_alloc(h, &dItems, 8ull * maxRows);
+  if (!rc) rc = scratch_alloc(h, &dRows, 4ull * kMlpRow * maxRows);
+  if (!rc) rc = scratch_alloc(h, &dCount, 16);
+  if (!rc) {
+    cudaMemcpyAsync(dT, targets, 4ull * nt, cudaMemcpyHostToDevice, h->stream);
+    const DevState S = h->state();
+    mlp_harvest(h->stream, S, (const uint32_t *)dT, nt, theta, band, h->params.epsilon,
+                (uint2 *)dItems, maxRows, (uint32_t *)dCount, (float *)dRows);
+    uint32_t cnt = 0;
+    cudaMemcpyAsync(&cnt, dCount, 4, cudaMemcpyDeviceToHost, h->stream);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+      rc = cuda_fail(h, e, "harvest");
+    } else {
+      cnt = std::min(cnt, maxRows);
+      e = cudaMemcpy(rows, dRows, 4ull * kMlpRow * cnt, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) rc = cuda_fail(h, e, "harvest copy");
+      *nRows = cnt;
+    }
+  }
+  for (void *p : {dT, dItems, dRows, dCount})
+    if (p) scratch_free(h, p);
+  return rc;
+}
+
+int nbx_mlp_gradient(nbx_handle *h, const float *rows, uint32_t n, float *grad,
+                     float *loss) {
+  if (!h || !rows || !n || !grad) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!h->mlpLoaded) return fail(h, NBX_ERR_STATE, "no MLP parameters");
+  const int blocks = (n + mlp_rows_per_block() - 1) / mlp_rows_per_block();
+  void *dRows = nullptr, *dPart = nullptr, *dLoss = nullptr;
+  int rc = scratch_alloc(h, &dRows, 4ull * kMlpRow * n);
+  if (!rc) rc = scratch_alloc(h, &dPart, 4ull * kMlpParams * blocks);
+  if (!rc) rc = scratch_alloc(h, &dLoss, 4ull * (blocks + 1));
+  if (!rc) {
+    cudaMemcpyAsync(dRows, rows, 4ull * kMlpRow * n, cudaMemcpyHostToDevice, h->stream);
+    mlp_gradient(h->stream, (float *)dRows, nullptr, 0, n, h->mlpP, (float *)dPart,
+                 (float *)dLoss, h->mlpGrad, h->mlpGrad + kMlpParams);
+    float out[kMlpParams + 1];
+    cudaMemcpyAsync(out, h->mlpGrad, sizeof out, cudaMemcpyDeviceToHost, h->stream);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = cuda_fail(h, e, "mlp gradient");
+    else {
+      std::memcpy(grad, out, 4ull * kMlpParams);
+      if (loss) *loss = out[kMlpParams] / (float)n;
+    }
+  }
+  for (void *p : {dRows, dPart, dLoss})
+    if (p) scratch_free(h, p);
+  return rc;
+}
+
+int nbx_mlp_train(nbx_handle *h, const float *rows, uint32_t n, uint32_t epochs,
+                  uint32_t batch, float lr, uint32_t seed, float *epochLoss) {
+  if (!h || !rows || !n || !batch || batch > n) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!h->mlpLoaded) {
+    int rc = nbx_mlp_init(h, seed);
+    if (rc) return rc;
+  }
+  const uint32_t steps = n / batch;
+  const int blocks = (batch + mlp_rows_per_block() - 1) / mlp_rows_per_block();
+  void *dRows = nullptr, *dOrder = nullptr, *dPart = nullptr, *dLoss = nullptr,
+       *dSteps = nullptr;
+  int rc = scratch_alloc(h, &dRows, 4ull * kMlpRow * n);
+  if (!rc) rc = scratch_alloc(h, &dOrder, 4ull * n);
+  if (!rc) rc = scratch_alloc(h, &dPart, 4ull * kMlpParams * blocks);
+  if (!rc) rc = scratch_alloc(h, &dLoss, 4ull * (blocks + 1));
+  if (!rc) rc = scratch_alloc(h, &dSteps, 4ull * steps);
+  if (!rc) {
+    cudaMemcpyAsync(dRows, rows, 4ull * kMlpRow * n, cudaMemcpyHostToDevice, h->stream);
+    std::vector<uint32_t> order(n);
+    std::vector<float> stepLoss(steps);
+    std::mt19937 rng(seed);
+    for (uint32_t e = 0; e < epochs && !rc; ++e) {
+      for (uint32_t i = 0; i < n; ++i) order[i] = i;
+      std::shuffle(order.begin(), order.end(), rng);
+      cudaMemcpyAsync(dOrder, order.data(), 4ull * n, cudaMemcpyHostToDevice, h->stream);
+      for (uint32_t k = 0; k < steps; ++k) {
+        mlp_gradient(h->stream, (float *)dRows, (uint32_t *)dOrder, k * batch, batch,
+                     h->mlpP, (float *)dPart, (float *)dLoss, h->mlpGrad,
+                     (float *)dSteps + k);
+        mlp_adam(h->stream, h->mlpP, h->mlpGrad, h->mlpM, h->mlpV, ++h->mlpStep, lr,
+                 h->mlpW);
+      }
+      cudaMemcpyAsync(stepLoss.data(), dSteps, 4ull * steps, cudaMemcpyDeviceToHost,
+                      h->stream);
+      cudaError_t ce = cudaStreamSynchronize(h->stream);
+      if (ce != cudaSuccess) rc = cuda_fail(h, ce, "mlp train");
+      if (epochLoss) {
+        double s = 0.0;
+        for (float v : stepLoss) s += v;
+        epochLoss[e] = (float)(s / ((double)steps * batch));
+      }
+    }
+  }
+  for (void *p : {dRows, dOrder, dPart, dLoss, dSteps})
+    if (p) scratch_free(h, p);
+  destroy_graphs(h);
+  return rc;
+}
+
+int nbx_mlp_eval(nbx_handle *h, const float *feat, uint32_t n, float *out,
+                 int tensor) {
+  if (!h || (n && (!feat || !out))) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!h->mlpLoaded) return fail(h, NBX_ERR_STATE, "no MLP parameters");
+  if (!n) return NBX_OK;
+  void *dF = nullptr, *dO = nullptr;
+  int rc = scratch_alloc(h, &dF, 36ull * n);
+  if (!rc) rc = scratch_alloc(h, &dO, 8ull * n);
+  if (!rc) {
+    cudaMemcpyAsync(dF, feat, 36ull * n, cudaMemcpyHostToDevice, h->stream);
+    mlp_eval(h->stream, (float *)dF, n, h->mlpP, h->mlpW, (float *)dO, tensor != 0);
+    cudaMemcpyAsync(out, dO, 8ull * n, cudaMemcpyDeviceToHost, h->stream);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = cuda_fail(h, e, "mlp eval");
+  }
+  for (void *p : {dF, dO})
+    if (p) scratch_free(h, p);
+  return rc;
 }
 
 int nbx_get_stream(nbx_handle *h, void **stream) {

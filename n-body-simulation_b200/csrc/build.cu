@@ -203,6 +203,7 @@ __global__ void k_levels(DevState S) {
       }
       G.nodeCount = nodes;
       G.levelCount = levels;
+      G.travCount = 0;
     }
     // block-wide exclusive scan of node counts -> node bases
     __shared__ uint32_t sScan[1024];
@@ -412,7 +413,9 @@ __global__ void __launch_bounds__(kBlock) k_upward(DevState S) {
     S.comX[g] = X;
     S.comY[g] = Y;
     S.moments[g] = make_float4(ixx, iyy, ixy, 0.0f);
-    S.subtree[g] = 1;
+    // empty leaves (no bodies) add nothing whether accepted or opened, so
+    // the traversal layout leaves them out
+    S.subtree[g] = b1 > b0 ? 1u : 0u;
     // climb (at most kMaxDepth levels; parent indices are range-checked)
     int32_t node = S.parent[g];
     for (int guard = 0; node >= 0 && guard <= kMaxDepth; ++guard) {
@@ -482,7 +485,8 @@ __global__ void __launch_bounds__(kBlock) k_preorder(DevState S) {
       for (uint32_t t = 0; t < q; ++t) pre += S.subtree[nb + cb + t];
       cur = p;
     }
-    if (pre >= G.nodeCount) continue;
+    if (g == nb) S.seg[sg].travCount = S.subtree[g];
+    if (S.subtree[g] == 0 || pre >= G.nodeCount) continue; // empty node
     const uint32_t pg = nb + pre;
     const float sz = S.size[g];
     S.tA[pg] = make_float4(S.comX[g], S.comY[g], S.mass[g], __fmul_rn(sz, sz));
@@ -490,6 +494,7 @@ __global__ void __launch_bounds__(kBlock) k_preorder(DevState S) {
                          (int)(G.start + S.end[g]), S.children[g] == 0 ? 1 : 0);
     const float4 mo = S.moments[g];
     S.tM[pg] = make_float4(mo.x, mo.y, mo.z, sz);
+    S.tC[pg] = make_float2(S.centerX[g], S.centerY[g]);
   }
 }
 

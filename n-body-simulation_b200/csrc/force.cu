@@ -21,6 +21,7 @@
 // the host-compiled reference traversal on the same tree.  kExact = false
 // lets the compiler contract and uses the hardware reciprocal
 // approximation (relative difference ~1e-7 per term).
+#include "mlp.cuh"
 #include "nbx_state.cuh"
 
 #include <float.h>
@@ -47,6 +48,17 @@ __device__ __forceinline__ float inv_sqrt_law(float x) {
   } else {
     return fast_inv_sqrt(x);
   }
+}
+
+// The tree force law's factor m * fastInvSqrt(d^2) / (d^2 + eps^2), clamped
+// to FLT_MAX (the term is d * factor).
+template <bool kExact>
+__device__ __forceinline__ float law_factor(float dSq, float m, float eSq) {
+  if (kExact)
+    return fminf(__fmul_rn(__fmul_rn(m, inv_sqrt_law<true>(dSq)),
+                           __frcp_rn(__fadd_rn(dSq, eSq))),
+                 FLT_MAX);
+  return fminf(m * inv_sqrt_law<false>(dSq) * rcp_approx(dSq + eSq), FLT_MAX);
 }
 
 // One interaction of the tree force law; accumulates into (ax, ay).
@@ -76,13 +88,48 @@ __device__ __forceinline__ float sq_dist(float dx, float dy) {
 
 // kCount: instead of writing accelerations, add the walk's far (accepted,
 // mass > 0), near (leaf body terms) and visited-node counts to counts[0..2].
-template <bool kExact, bool kCount = false>
+// Second-order (quadrupole) term of the softened law for a cell with mass
+// M and second moments I about its centre of mass, relative to the kernel
+// g(r) = 1/(r (r^2 + eps^2)) of the monopole M g d:
+//   delta = 1/2 [ (g'/r)(2 I d + tr(I) d) + (g''/r^2 - g'/r^3) d (d'Id) ],
+// returned divided by M g so that the cell term is fac * (d + delta/(M g)).
+__device__ __forceinline__ void quad_term(float dx, float dy, float dSq,
+                                          float eSq, float mass, float ixx,
+                                          float iyy, float ixy, float &qx,
+                                          float &qy) {
+  const float q = dSq + eSq;
+  const float iq = 1.0f / q, ir2 = 1.0f / dSq;
+  const float c3 = 3.0f * dSq + eSq;
+  const float aOverG = -c3 * ir2 * iq;                        // g'/(r g)
+  const float gpp = -6.0f * iq + c3 * (2.0f * ir2 * iq + 4.0f * iq * iq);
+  const float bOverG = gpp * ir2 + c3 * ir2 * ir2 * iq;       // B / g
+  const float Idx = ixx * dx + ixy * dy, Idy = ixy * dx + iyy * dy;
+  const float tr = ixx + iyy;
+  const float dId = dx * Idx + dy * Idy;
+  const float h = 0.5f / mass;
+  qx = h * (aOverG * (2.0f * Idx + tr * dx) + bOverG * dx * dId);
+  qy = h * (aOverG * (2.0f * Idy + tr * dy) + bOverG * dy * dId);
+}
+
+// kCorr = 1: accepted cells with size^2 >= d^2 * band^2 get the learned
+// correction (mlp.cuh), evaluated for the warp's rows on tensor cores;
+// kCorr = 2: they get the analytic quadrupole term instead (the control).
+template <bool kExact, bool kCount = false, int kCorr = 0>
 __global__ void __launch_bounds__(kForceBlock)
     k_forces(DevState S, float tSq, float eSq,
-             unsigned long long *counts = nullptr) {
+             unsigned long long *counts = nullptr,
+             const MlpDev *__restrict__ mlp = nullptr, float bandSq = 0.0f,
+             float eps = 0.0f) {
   __shared__ float4 sA[kWarps][32];
   __shared__ int4 sB[kWarps][32];
   __shared__ float4 sBody[kWarps][32];
+  __shared__ MlpDev sW;
+  __shared__ __nv_bfloat16 sStage[kCorr == 1 ? kWarps : 1][32][16];
+  if (kCorr == 1) {
+    for (int q = threadIdx.x; q < (int)(sizeof(MlpDev) / 4); q += blockDim.x)
+      reinterpret_cast<uint32_t *>(&sW)[q] = reinterpret_cast<const uint32_t *>(mlp)[q];
+    __syncthreads();
+  }
   const int lane = threadIdx.x & 31;
   const int w = threadIdx.x >> 5;
   const uint32_t totalNodes = S.counters[4];
@@ -98,9 +145,9 @@ __global__ void __launch_bounds__(kForceBlock)
       x = b.x;
       y = b.y;
       const SegDev &G = S.seg[S.segOf[i]];
-      if (G.nodeCount > 0) {
+      if (G.travCount > 0) {
         cur = G.nodeBase;
-        endNode = G.nodeBase + G.nodeCount;
+        endNode = G.nodeBase + G.travCount;
       }
     }
     float ax = 0.0f, ay = 0.0f;
@@ -133,9 +180,48 @@ __global__ void __launch_bounds__(kForceBlock)
       const bool accept = at && A.w < far;
       const bool openLeaf = at && !accept && B.w != 0;
       {
-        float tx = ax, ty = ay;
-        add_term<kExact>(dx, dy, dSq, A.z, eSq, tx, ty);
         const bool use = accept && A.z > 0.0f;
+        const float fac = law_factor<kExact>(dSq, A.z, eSq);
+        float tx, ty;
+        if (kExact) {
+          tx = __fadd_rn(ax, __fmul_rn(dx, fac));
+          ty = __fadd_rn(ay, __fmul_rn(dy, fac));
+        } else {
+          tx = fmaf(dx, fac, ax);
+          ty = fmaf(dy, fac, ay);
+        }
+        if (kCorr == 2) {
+          const bool band = use && A.w >= dSq * bandSq;
+          if (__ballot_sync(0xffffffffu, band)) {
+            const float4 M = S.tM[k];
+            float qx, qy;
+            quad_term(dx, dy, dSq, eSq, A.z, M.x, M.y, M.z, qx, qy);
+            if (band) {
+              tx = ax + fac * (dx + qx);
+              ty = ay + fac * (dy + qy);
+            }
+          }
+        }
+        if (kCorr == 1) {
+          const bool band = use && A.w >= dSq * bandSq;
+          if (__ballot_sync(0xffffffffu, band)) {
+            const float4 M = S.tM[k];
+            const float2 Q = S.tC[k];
+            float f[9], ux = 0.0f, uy = 0.0f;
+            bool ok = band && mlp_features(dx, dy, dSq, A.z, M.w, Q.x, Q.y, A.x,
+                                           A.y, M.x, M.y, M.z, 1.0f, eps, f, ux, uy);
+            if (!ok)
+              for (int q = 0; q < 9; ++q) f[q] = 0.0f;
+            float o0, o1;
+            mlp_warp(sW, f, sStage[w], o0, o1);
+            if (ok) {
+              // |mono| * ((1 + t0) u + t1 w), w = (-uy, ux)
+              const float r = dSq * rsqrtf(dSq);
+              tx = ax + fac * (dx * (1.0f + o0) - r * o1 * uy);
+              ty = ay + fac * (dy * (1.0f + o0) + r * o1 * ux);
+            }
+          }
+        }
         ax = use ? tx : ax;
         ay = use ? ty : ay;
         if (kCount) nFar += use ? 1u : 0u;
@@ -239,13 +325,20 @@ double fp32_fma_peak_tflops(cudaStream_t s) {
   return ms > 0 ? flops / (ms * 1e-3) / 1e12 : 0.0;
 }
 
-void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks) {
+void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
+                   const MlpDev *mlp, float band, int corr) {
   if (blocks <= 0) {
     uint32_t warps = (S.n + 31) / 32;
     uint32_t b = (warps + kWarps - 1) / kWarps;
     blocks = (int)(b ? b : 1);
   }
-  if (exact)
+  if (corr == 1 && mlp)
+    k_forces<false, false, 1><<<blocks, kForceBlock, 0, s>>>(
+        S, S.tSq, S.eSq, nullptr, mlp, band * band, sqrtf(S.eSq));
+  else if (corr == 2)
+    k_forces<false, false, 2><<<blocks, kForceBlock, 0, s>>>(
+        S, S.tSq, S.eSq, nullptr, nullptr, band * band, sqrtf(S.eSq));
+  else if (exact)
     k_forces<true><<<blocks, kForceBlock, 0, s>>>(S, S.tSq, S.eSq);
   else
     k_forces<false><<<blocks, kForceBlock, 0, s>>>(S, S.tSq, S.eSq);

@@ -19,7 +19,8 @@ struct SegDev {
   uint32_t nodeCount; // nodes in this segment's tree
   uint32_t levelCount;
   uint32_t largeStart, largeCount;
-  uint32_t pad2[3];
+  uint32_t travCount; // nodes in the traversal layout (non-empty nodes)
+  uint32_t pad2[2];
 };
 
 constexpr int kMaxDepth = 32;   // TreeKernels.cuh:29
@@ -101,6 +102,7 @@ struct DevState {
   float4 *tA; // {comX, comY, mass, size*size}
   int4 *tB;   // {next (preorder, global), start, end, isLeaf}
   float4 *tM; // {Ixx, Iyy, Ixy, size} for the learned correction
+  float2 *tC; // square centre, for the learned correction
 };
 
 } // namespace nbx

@@ -33,8 +33,12 @@ EXPORTS = (
     "nbx_energy_momentum_fp64", "nbx_status_bits", "nbx_last_error",
     "nbx_uniform_disc", "nbx_two_discs", "nbx_cold_square", "nbx_version",
     "nbx_get_stream", "nbx_step_kernel_count", "nbx_interaction_count",
-    "nbx_fp32_peak_tflops", "nbx_profile_step",
+    "nbx_fp32_peak_tflops", "nbx_profile_step", "nbx_mlp_set_params",
+    "nbx_mlp_get_params", "nbx_mlp_init", "nbx_mlp_harvest", "nbx_mlp_train",
+    "nbx_mlp_gradient", "nbx_mlp_eval",
 )
+MLP_PARAMS = 1442
+MLP_ROW = 12
 
 PHASE = {"iterate": 0, "collide": 1, "build": 2, "forces": 3, "attract": 4,
          "step": 5}
@@ -48,7 +52,8 @@ class Params(C.Structure):
                 ("leaf_capacity", C.c_int32), ("collisions", C.c_int32),
                 ("exact_math", C.c_int32), ("use_mlp", C.c_int32),
                 ("node_factor", C.c_float), ("pair_factor", C.c_float),
-                ("force_blocks", C.c_int32), ("device", C.c_int32)]
+                ("force_blocks", C.c_int32), ("device", C.c_int32),
+                ("mlp_band", C.c_float)]
 
 
 class NbxError(RuntimeError):
@@ -105,6 +110,15 @@ def lib() -> C.CDLL:
         "nbx_interaction_count": [vp, f64p],
         "nbx_fp32_peak_tflops": [C.POINTER(C.c_double)],
         "nbx_profile_step": [vp, C.c_uint32, vp, vp, C.POINTER(C.c_uint32)],
+        "nbx_mlp_set_params": [vp, vp, C.c_uint32],
+        "nbx_mlp_get_params": [vp, vp, C.c_uint32],
+        "nbx_mlp_init": [vp, C.c_uint32],
+        "nbx_mlp_harvest": [vp, vp, C.c_uint32, C.c_float, C.c_float, vp,
+                            C.c_uint32, C.POINTER(C.c_uint32)],
+        "nbx_mlp_train": [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
+                          C.c_uint32, vp],
+        "nbx_mlp_gradient": [vp, vp, C.c_uint32, vp, vp],
+        "nbx_mlp_eval": [vp, vp, C.c_uint32, vp, C.c_int],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -307,6 +321,51 @@ class Handle:
         raw = labels.raw
         return {raw[32 * k: 32 * k + 32].split(b"\0")[0].decode(): float(ms[k])
                 for k in range(cnt.value)}
+
+    # -- learned far-field correction --------------------------------
+    def mlp_set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.size == MLP_PARAMS
+        self._c(lib().nbx_mlp_set_params(self.h, p.ctypes.data, MLP_PARAMS))
+
+    def mlp_get_params(self) -> np.ndarray:
+        p = np.zeros(MLP_PARAMS, np.float32)
+        self._c(lib().nbx_mlp_get_params(self.h, p.ctypes.data, MLP_PARAMS))
+        return p
+
+    def mlp_init(self, seed: int = 0):
+        self._c(lib().nbx_mlp_init(self.h, seed))
+
+    def mlp_harvest(self, targets, theta: float, band: float,
+                    max_rows: int = 1 << 20) -> np.ndarray:
+        t = np.ascontiguousarray(targets, np.uint32)
+        rows = np.zeros((max_rows, MLP_ROW), np.float32)
+        cnt = C.c_uint32()
+        self._c(lib().nbx_mlp_harvest(self.h, t.ctypes.data, len(t), theta, band,
+                                      rows.ctypes.data, max_rows, C.byref(cnt)))
+        return rows[:cnt.value]
+
+    def mlp_train(self, rows, epochs=10, batch=4096, lr=1e-3, seed=0):
+        r = np.ascontiguousarray(rows, np.float32)
+        losses = np.zeros(epochs, np.float32)
+        self._c(lib().nbx_mlp_train(self.h, r.ctypes.data, len(r), epochs, batch,
+                                    lr, seed, losses.ctypes.data))
+        return losses
+
+    def mlp_gradient(self, rows):
+        r = np.ascontiguousarray(rows, np.float32)
+        g = np.zeros(MLP_PARAMS, np.float32)
+        loss = C.c_float()
+        self._c(lib().nbx_mlp_gradient(self.h, r.ctypes.data, len(r), g.ctypes.data,
+                                       C.byref(loss)))
+        return g, loss.value
+
+    def mlp_eval(self, features, tensor_cores=True):
+        f = np.ascontiguousarray(features, np.float32).reshape(-1, 9)
+        out = np.zeros((len(f), 2), np.float32)
+        self._c(lib().nbx_mlp_eval(self.h, f.ctypes.data, len(f), out.ctypes.data,
+                                   int(tensor_cores)))
+        return out
 
     def status_bits(self) -> int:
         b = C.c_uint32()
