@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=N_BODIES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true",
+                    help="headline workload only (no learned/ensemble legs)")
     return ap.parse_args()
 
 
@@ -193,6 +195,114 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------- extra legs
+WEIGHTS = os.path.join(PKG, "weights", "farfield_mlp.f32")
+
+
+def time_steps(torch, h, stream, steps):
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    h.sync()
+    e0.record(stream)
+    h.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    h.sync()
+    return e0.elapsed_time(e1) / steps
+
+
+def forms_leg(nbx, torch, sim, n, local, ids, args):
+    """Plain theta 0.5 vs the learned correction (and the analytic
+    quadrupole control) on the same state: body-steps/s and the force error
+    against the FP64 direct sum on the same 4096 sampled bodies."""
+    state = sim.download()
+    pos = np.empty(n, np.int64)
+    pos[state["id"]] = np.arange(n)
+    tg = pos[ids].astype(np.uint32)
+    weights = np.fromfile(WEIGHTS, "<f4")
+    steps = max(5, min(args.steps, 200))
+    out = []
+    for name, theta, use, band in (("plain", 0.5, 0, 0.5), ("learned", 0.7, 1, 0.5),
+                                   ("learned", 0.9, 1, 0.5), ("quadrupole", 0.7, 2, 0.5),
+                                   ("quadrupole", 0.5, 2, 0.3)):
+        h = nbx.Simulation(state, theta=theta, use_mlp=use, mlp_band=band, device=local)
+        if use == 1:
+            h.mlp_set_params(weights)
+        h.phase("attract")
+        err, _ = h.force_error(tg)
+        stream = torch.cuda.ExternalStream(h.stream(), device=local)
+        h.step(2)
+        ms = time_steps(torch, h, stream, steps)
+        out.append({"form": name, "theta": theta, "band": band,
+                    "body_steps_per_s": n / (ms * 1e-3), "ms_per_step": ms,
+                    "p50": err["median"], "p99": err["p99"], "steps": steps})
+        h.close()
+    return out
+
+
+def ensemble_leg(nbx, torch, world, rank, local, dist, args):
+    """512 discs of log-uniform size in [2000, 200000] advanced by one
+    handle, against looping the single-instance solver over the same
+    instances (one handle and captured graph per instance, launched
+    back to back without host synchronisation between instances)."""
+    sys.path.insert(0, PKG)
+    import ensemble
+    sizes = nbx.ensemble_sizes(512)
+    mine = ensemble.partition_instances(sizes, world)[rank]
+    my_sizes = sizes[mine]
+    bodies = np.concatenate([nbx.uniform_disc(int(sizes[i]), i) for i in mine])
+    steps = max(3, min(args.steps, 10))
+    h = nbx.Handle(my_sizes, theta=0.5, device=local)
+    h.upload(bodies)
+    stream = torch.cuda.ExternalStream(h.stream(), device=local)
+    h.step(2)
+    kernels = h.step_kernels()
+    ms = max_over_ranks(dist, local, time_steps(torch, h, stream, steps))
+    h.close()
+    total = int(sizes.sum())
+    res = {"instances": int(len(sizes)), "bodies": total, "theta": 0.5,
+           "steps": steps, "ms_per_step": ms,
+           "body_steps_per_s": total / (ms * 1e-3),
+           "kernels_per_step": kernels}
+    if world == 1:
+        loop_steps = 3
+        hs = []
+        start = 0
+        for i, nb in enumerate(sizes):
+            hi = nbx.Simulation(bodies[start:start + int(nb)], theta=0.5, device=local)
+            hi.step(1)
+            hs.append(hi)
+            start += int(nb)
+        for hi in hs:
+            hi.sync()
+        torch.cuda.synchronize(local)
+        # sequential loop: each instance's step completes before the next
+        # one starts, as a driver looping Simulation::step over instances
+        t0 = time.perf_counter()
+        for _ in range(loop_steps):
+            for hi in hs:
+                hi.step(1)
+                hi.sync()
+        seq_ms = (time.perf_counter() - t0) * 1e3 / loop_steps
+        # concurrent loop: all instances' step graphs enqueued back to back
+        # on their own streams, one synchronisation at the end
+        t0 = time.perf_counter()
+        for _ in range(loop_steps):
+            for hi in hs:
+                hi.step(1)
+        for hi in hs:
+            hi.sync()
+        loop_ms = (time.perf_counter() - t0) * 1e3 / loop_steps
+        for hi in hs:
+            hi.close()
+        res["looped_ms_per_step"] = seq_ms
+        res["looped_body_steps_per_s"] = total / (seq_ms * 1e-3)
+        res["speedup_vs_looped"] = seq_ms / ms
+        res["looped_concurrent_ms_per_step"] = loop_ms
+        res["speedup_vs_looped_concurrent"] = loop_ms / ms
+    return res
+
+
 # ------------------------------------------------------------------ b200
 def run_b200(args):
     world, rank, local, dist = dist_setup(args)
@@ -274,6 +384,10 @@ def run_b200(args):
     e2e_ms = max_over_ranks(dist, local, e2e_ms)
     e2e_value = world * n / (e2e_ms * 1e-3)
 
+    learned = forms_leg(nbx, torch, sim, n, local, ids, args) if not args.quick else None
+    sim_keep = sim
+    ens = ensemble_leg(nbx, torch, world, rank, local, dist, args) if not args.quick else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -312,11 +426,15 @@ def run_b200(args):
         "gpu_launches": kernels_per_step * args.steps,
         "clocks": clk,
     }
+    if learned is not None:
+        line["learned_theta"] = learned
+    if ens is not None:
+        line["ensemble"] = ens
     if cpu is not None:
         line["cpu_baseline"] = cpu
     if rank == 0:
         print(json.dumps(line), flush=True)
-    sim.close()
+    sim_keep.close()
     if dist is not None:
         dist.destroy_process_group()
 

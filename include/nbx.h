@@ -245,6 +245,16 @@ int nbx_mlp_gradient(nbx_handle *h, const float *rows, uint32_t n_rows,
 int nbx_mlp_eval(nbx_handle *h, const float *features, uint32_t n, float *out,
                  int tensor_cores);
 
+/* --- autotuner (no counterpart in the reference) ---
+ * Times `steps` steps from the current state for each candidate -- force
+ * launch grids {one warp per 32 bodies, 4, 8 or 16 blocks per SM} and, if
+ * allow_leaf, leaf capacities {8, 12, 16, 24, 32} (a leaf capacity other
+ * than 16 changes the tree, so results then differ from the reference's) --
+ * keeps the fastest in the handle's parameters, and restores the state.
+ * *best receives the chosen parameters, *best_ms their time per step. */
+int nbx_autotune(nbx_handle *h, int allow_leaf, uint32_t steps,
+                 nbx_params *best, float *best_ms);
+
 /* --- host-side scenario generators (product host code) --- */
 
 /* uniformDisc(n, seed): src/Utils.cpp:6-54. */
@@ -261,6 +271,11 @@ int nbx_two_discs(uint32_t n, uint32_t seed, float approach_fraction,
 /* n unit-mass, radius-1 bodies at rest uniform in [-h, h]^2 with
  * h = 3*sqrt(n), mt19937(seed) (viewer/Scenarios.cpp:50-57). */
 int nbx_cold_square(uint32_t n, uint32_t seed, nbx_body *out);
+
+/* Instance sizes of the batched ensemble: instance i has
+ * round(exp(U(ln lo, ln hi))) bodies, U drawn from mt19937(i). */
+int nbx_ensemble_sizes(uint32_t count, uint32_t lo, uint32_t hi,
+                       uint32_t *sizes);
 
 /* Library build/version string. */
 const char *nbx_version(void);

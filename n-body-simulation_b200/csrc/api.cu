@@ -1075,6 +1075,93 @@ int nbx_mlp_eval(nbx_handle *h, const float *feat, uint32_t n, float *out,
   return rc;
 }
 
+// ------------------------------------------------------------ autotuner
+int nbx_autotune(nbx_handle *h, int allowLeaf, uint32_t steps, nbx_params *best,
+                 float *bestMs) {
+  if (!h || !best || steps == 0) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!h->uploaded) return fail(h, NBX_ERR_STATE, "no bodies uploaded");
+  if (h->n == 0) {
+    *best = h->params;
+    if (bestMs) *bestMs = 0.0f;
+    return NBX_OK;
+  }
+  // snapshot of the state: every trial starts from it, and it is restored
+  const DevState S0 = h->state();
+  const size_t n = h->n;
+  void *sv = nullptr;
+  int rc = scratch_alloc(h, &sv, n * (sizeof(float4) + sizeof(float2) * 2 + 4));
+  if (rc) return rc;
+  char *b = (char *)sv;
+  float4 *pv = (float4 *)b;
+  float2 *mr = (float2 *)(b + n * 16), *acc = (float2 *)(b + n * 24);
+  uint32_t *id = (uint32_t *)(b + n * 32);
+  const int cur0 = h->cur;
+  auto save = [&]() {
+    cudaMemcpyAsync(pv, S0.pv, n * 16, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(mr, S0.mr, n * 8, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(acc, S0.acc, n * 8, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(id, S0.id, n * 4, cudaMemcpyDeviceToDevice, h->stream);
+  };
+  auto restore = [&]() {
+    h->cur = cur0;
+    cudaMemcpyAsync(S0.pv, pv, n * 16, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(S0.mr, mr, n * 8, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(S0.acc, acc, n * 8, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(S0.id, id, n * 4, cudaMemcpyDeviceToDevice, h->stream);
+  };
+  save();
+  const nbx_params start = h->params;
+  std::vector<int> leaves = {start.leaf_capacity};
+  if (allowLeaf) leaves = {8, 12, 16, 24, 32};
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+  const int grids[] = {0, sms * 4, sms * 8, sms * 16};
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  nbx_params bestP = start;
+  float bestT = 1e30f;
+  for (int leaf : leaves) {
+    for (int grid : grids) {
+      nbx_params p = start;
+      p.leaf_capacity = leaf;
+      p.force_blocks = grid;
+      h->params = p;
+      sync_params(h);
+      destroy_graphs(h);
+      restore();
+      if ((rc = nbx_step(h, 1)) != NBX_OK) break;
+      cudaEventRecord(e0, h->stream);
+      if ((rc = nbx_step(h, steps)) != NBX_OK) break;
+      cudaEventRecord(e1, h->stream);
+      if ((rc = nbx_sync(h)) != NBX_OK) break;
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms /= (float)steps;
+      if (ms < bestT) {
+        bestT = ms;
+        bestP = p;
+      }
+    }
+    if (rc) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->params = rc ? start : bestP;
+  sync_params(h);
+  destroy_graphs(h);
+  restore();
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  scratch_free(h, sv);
+  if (e != cudaSuccess && !rc) rc = cuda_fail(h, e, "autotune");
+  h->treeValid = false;
+  h->collideValid = false;
+  *best = h->params;
+  if (bestMs) *bestMs = bestT;
+  return rc;
+}
+
 int nbx_get_stream(nbx_handle *h, void **stream) {
   if (!h || !stream) return NBX_ERR_ARG;
   *stream = (void *)h->stream;

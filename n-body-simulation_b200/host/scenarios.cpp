@@ -109,3 +109,16 @@ extern "C" int nbx_cold_square(uint32_t n, uint32_t seed, nbx_body *out) {
   }
   return NBX_OK;
 }
+
+// Instance sizes of the batched ensemble: N_i = round(exp(U(ln lo, ln hi)))
+// drawn from mt19937(i) for instance i.
+extern "C" int nbx_ensemble_sizes(uint32_t count, uint32_t lo, uint32_t hi,
+                                  uint32_t *sizes) {
+  if ((count && !sizes) || lo == 0 || hi < lo) return NBX_ERR_ARG;
+  for (uint32_t i = 0; i < count; ++i) {
+    std::mt19937 rng(i);
+    std::uniform_real_distribution<double> u(std::log((double)lo), std::log((double)hi));
+    sizes[i] = (uint32_t)std::llround(std::exp(u(rng)));
+  }
+  return NBX_OK;
+}

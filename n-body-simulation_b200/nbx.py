@@ -35,7 +35,7 @@ EXPORTS = (
     "nbx_get_stream", "nbx_step_kernel_count", "nbx_interaction_count",
     "nbx_fp32_peak_tflops", "nbx_profile_step", "nbx_mlp_set_params",
     "nbx_mlp_get_params", "nbx_mlp_init", "nbx_mlp_harvest", "nbx_mlp_train",
-    "nbx_mlp_gradient", "nbx_mlp_eval",
+    "nbx_mlp_gradient", "nbx_mlp_eval", "nbx_ensemble_sizes", "nbx_autotune",
 )
 MLP_PARAMS = 1442
 MLP_ROW = 12
@@ -119,6 +119,9 @@ def lib() -> C.CDLL:
                           C.c_uint32, vp],
         "nbx_mlp_gradient": [vp, vp, C.c_uint32, vp, vp],
         "nbx_mlp_eval": [vp, vp, C.c_uint32, vp, C.c_int],
+        "nbx_ensemble_sizes": [C.c_uint32, C.c_uint32, C.c_uint32, vp],
+        "nbx_autotune": [vp, C.c_int, C.c_uint32, C.POINTER(Params),
+                         C.POINTER(C.c_float)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -160,6 +163,17 @@ def cold_square(n: int, seed: int = 0) -> np.ndarray:
     b = np.zeros(n, BODY_DTYPE)
     _check(None, lib().nbx_cold_square(n, seed, b))
     return b
+
+
+def ensemble_sizes(count: int, lo: int = 2000, hi: int = 200000) -> np.ndarray:
+    s = np.zeros(count, np.uint32)
+    _check(None, lib().nbx_ensemble_sizes(count, lo, hi, s.ctypes.data))
+    return s
+
+
+def ensemble_bodies(sizes) -> np.ndarray:
+    """Instance i is uniformDisc(sizes[i], seed i); instances back to back."""
+    return np.concatenate([uniform_disc(int(n), i) for i, n in enumerate(sizes)])
 
 
 def _check(h, rc):
@@ -321,6 +335,14 @@ class Handle:
         raw = labels.raw
         return {raw[32 * k: 32 * k + 32].split(b"\0")[0].decode(): float(ms[k])
                 for k in range(cnt.value)}
+
+    def autotune(self, allow_leaf=False, steps=3):
+        p = Params()
+        ms = C.c_float()
+        self._c(lib().nbx_autotune(self.h, int(allow_leaf), steps, C.byref(p),
+                                   C.byref(ms)))
+        return {"leaf_capacity": p.leaf_capacity, "force_blocks": p.force_blocks,
+                "ms_per_step": ms.value}
 
     # -- learned far-field correction --------------------------------
     def mlp_set_params(self, params):

@@ -1,0 +1,91 @@
+"""Batched ensemble: many instances of uneven size in one handle (one launch
+per phase for all of them) give exactly the single-instance results."""
+import numpy as np
+import pytest
+
+from conftest import same_bits
+
+pytestmark = pytest.mark.gpu
+
+
+def test_ensemble_equals_looped_instances(nbx, oracle):
+    sizes = nbx.ensemble_sizes(24, 200, 20000)
+    bodies = nbx.ensemble_bodies(sizes)
+    ens = nbx.Handle(sizes, exact_math=1, theta=0.5)
+    ens.upload(bodies)
+    ens.step(5)
+    ens.sync()
+    got = ens.download(id_order=True)
+    start = 0
+    for i, n in enumerate(sizes):
+        n = int(n)
+        sim = nbx.Simulation(bodies[start:start + n], exact_math=1, theta=0.5)
+        sim.step(5)
+        one = sim.download(id_order=True)
+        sim.close()
+        assert same_bits(got[start:start + n], one), i
+        if i < 3:  # and against the CPU oracle
+            ref = np.sort(oracle.step(bodies[start:start + n], steps=5, theta=0.5),
+                          order="id")
+            assert same_bits(one, ref), i
+        start += n
+    ens.close()
+
+
+def test_ensemble_introspection_per_instance(nbx, oracle):
+    sizes = nbx.ensemble_sizes(6, 500, 5000)
+    bodies = nbx.ensemble_bodies(sizes)
+    ens = nbx.Handle(sizes)
+    ens.upload(bodies)
+    ens.phase("build")
+    start = 0
+    for i, n in enumerate(sizes):
+        n = int(n)
+        b = bodies[start:start + n]
+        codes, perm = ens.morton(i)
+        root, ocodes, operm, sb, tree = oracle.morton_build(b)
+        assert np.array_equal(codes, ocodes) and np.array_equal(perm, operm)
+        t = ens.tree(i)
+        for k, v in tree.trimmed().items():
+            assert same_bits(t[k], v), (i, k)
+        start += n
+    ens.close()
+
+
+def test_ensemble_collisions_and_fast_math(nbx):
+    sizes = nbx.ensemble_sizes(8, 1000, 8000)
+    bodies = nbx.ensemble_bodies(sizes)
+    ens = nbx.Handle(sizes, theta=0.5)
+    ens.upload(bodies)
+    ens.step(40)
+    ens.sync()
+    got = ens.download(id_order=True)
+    start = 0
+    for i, n in enumerate(sizes):
+        n = int(n)
+        sim = nbx.Simulation(bodies[start:start + n], theta=0.5)
+        sim.step(40)
+        assert same_bits(got[start:start + n], sim.download(id_order=True)), i
+        sim.close()
+        start += n
+    ens.close()
+
+
+def test_autotune_restores_state(nbx):
+    sizes = nbx.ensemble_sizes(16, 1000, 20000)
+    bodies = nbx.ensemble_bodies(sizes)
+    h = nbx.Handle(sizes, theta=0.5)
+    h.upload(bodies)
+    h.step(2)
+    before = h.download()
+    best = h.autotune(allow_leaf=False, steps=2)
+    assert best["leaf_capacity"] == 16 and best["ms_per_step"] > 0
+    assert same_bits(h.download(), before)
+    # stepping with the tuned launch gives the reference results
+    h.step(3)
+    ref = nbx.Handle(sizes, theta=0.5)
+    ref.upload(bodies)
+    ref.step(5)
+    assert same_bits(h.download(), ref.download())
+    h.close()
+    ref.close()
