@@ -166,6 +166,24 @@ int nbx_get_pairs(nbx_handle *h, int32_t *later, int32_t *earlier,
 int nbx_direct_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m,
                     double *ax, double *ay);
 
+/* nbx_direct_fp64 for callers that cannot allocate device memory (their
+ * memory belongs to another allocator or is budgeted at start-up, or they
+ * must not pay cudaMalloc's device-wide synchronisation inside a loop).  No
+ * counterpart in the reference.  Every pointer is DEVICE memory owned by
+ * the caller: body positions x, y and masses (n floats each, the bodies'
+ * current order), targets (m indices), outputs ax, ay (m doubles); runs on
+ * `stream` (cudaStream_t, NULL = default stream) on the current device.
+ * Allocates nothing: its partial sums live in a fixed 4 MiB device array of
+ * the library, held by every GPU that loads it until exit.  At most 4096
+ * targets per call (NBX_ERR_CAPACITY beyond).  The first call on a device
+ * looks up that array's address; make it before any stream capture.  Calls
+ * share the array: calls whose kernels overlap on the GPU race, so order
+ * them on one stream. */
+int nbx_direct_fp64_noalloc(const float *x, const float *y, const float *mass,
+                            uint32_t n, const uint32_t *targets, uint32_t m,
+                            double epsilon, double *ax, double *ay,
+                            void *stream);
+
 /* Relative force error of the last force pass against nbx_direct_fp64 for
  * the given targets: stats = {median, p99, max, mean}; per-target errors
  * are written to err if not NULL.  (CheckCuda.cu:580-625) */

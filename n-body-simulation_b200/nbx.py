@@ -36,6 +36,7 @@ EXPORTS = (
     "nbx_fp32_peak_tflops", "nbx_profile_step", "nbx_mlp_set_params",
     "nbx_mlp_get_params", "nbx_mlp_init", "nbx_mlp_harvest", "nbx_mlp_train",
     "nbx_mlp_gradient", "nbx_mlp_eval", "nbx_ensemble_sizes", "nbx_autotune",
+    "nbx_direct_fp64_noalloc",
 )
 MLP_PARAMS = 1442
 MLP_ROW = 12
@@ -122,6 +123,8 @@ def lib() -> C.CDLL:
         "nbx_ensemble_sizes": [C.c_uint32, C.c_uint32, C.c_uint32, vp],
         "nbx_autotune": [vp, C.c_int, C.c_uint32, C.POINTER(Params),
                          C.POINTER(C.c_float)],
+        "nbx_direct_fp64_noalloc": [vp, vp, vp, C.c_uint32, vp, C.c_uint32,
+                                    C.c_double, vp, vp, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
