@@ -158,6 +158,27 @@ int nbx_get_tree(nbx_handle *h, uint32_t instance, float *com_x, float *com_y,
 int nbx_get_pairs(nbx_handle *h, int32_t *later, int32_t *earlier,
                   int64_t capacity, int64_t *count);
 
+/* Accelerations at arbitrary points (px[i], py[i]) from instance 0's last
+ * tree, with the handle's theta/epsilon: QuadTree::acceleration(pos, bodies)
+ * for any position (QuadTree.h:83-85, QuadTree.cpp:264-389). */
+int nbx_accel_at(nbx_handle *h, const float *px, const float *py, uint32_t n,
+                 float *ax, float *ay);
+
+/* --- NBS2 trajectory files (Main.cpp:13-49, load_sim.py:1-28) ---
+ * 28-byte header "NBS2", n_bodies, total_steps, output_every, num_frames =
+ * 1 + total_steps / output_every, completed_frames, dt; then float32
+ * mass[n] and radius[n] in id order; then frames of n records
+ * {x, y, vx, vy} in id order.  completed_frames is rewritten in place after
+ * every frame, so a killed run stays readable. */
+typedef struct nbx_nbs2 nbx_nbs2;
+int nbx_nbs2_open(const char *path, uint32_t n, uint32_t total_steps,
+                  uint32_t output_every, float dt, const float *mass_by_id,
+                  const float *radius_by_id, nbx_nbs2 **out);
+/* One frame from body records in id order (nbx_download_bodies with
+ * id_order = 1). */
+int nbx_nbs2_write_frame(nbx_nbs2 *f, const nbx_body *bodies_by_id);
+int nbx_nbs2_close(nbx_nbs2 *f);
+
 /* --- FP64 checks --- */
 
 /* FP64 direct-sum accelerations with the tree's force law (no softening

@@ -38,6 +38,8 @@ int mlp_rows_per_block();
 void launch_interaction_count(cudaStream_t s, const DevState &S,
                               unsigned long long *counts);
 double fp32_fma_peak_tflops(cudaStream_t s);
+void launch_query_forces(cudaStream_t s, const DevState &S, bool exact,
+                         const float2 *query, uint32_t nq, float2 *out);
 void launch_direct_fp64(cudaStream_t s, const float4 *pv, const float2 *mr,
                         uint32_t n, const uint32_t *targets, uint32_t m,
                         double eps, double2 *partial, double *ax, double *ay);
@@ -238,6 +240,8 @@ int allocate(nbx_handle *h) {
   A(S.plist, S.pairCapacity);
   A(S.plistTmp, S.pairCapacity);
   A(S.twin, S.pairCapacity);
+  A(S.stash, (size_t)n * 16);
+  A(S.largePairs, n + 64);
   A(S.fillLarge, n);
   A(S.nLater, n);
   A(S.unitFlag, n);
@@ -1073,6 +1077,31 @@ int nbx_mlp_eval(nbx_handle *h, const float *feat, uint32_t n, float *out,
   for (void *p : {dF, dO})
     if (p) scratch_free(h, p);
   return rc;
+}
+
+int nbx_accel_at(nbx_handle *h, const float *px, const float *py, uint32_t nq,
+                 float *ax, float *ay) {
+  if (!h || (nq && (!px || !py || !ax || !ay))) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
+  if (nq == 0) return NBX_OK;
+  std::vector<float2> q(nq), r(nq);
+  for (uint32_t i = 0; i < nq; ++i) q[i] = make_float2(px[i], py[i]);
+  void *buf = nullptr;
+  int rc = scratch_alloc(h, &buf, 16ull * nq);
+  if (rc) return rc;
+  float2 *dq = (float2 *)buf, *dr = dq + nq;
+  cudaMemcpyAsync(dq, q.data(), 8ull * nq, cudaMemcpyHostToDevice, h->stream);
+  launch_query_forces(h->stream, h->state(), h->params.exact_math != 0, dq, nq, dr);
+  cudaMemcpyAsync(r.data(), dr, 8ull * nq, cudaMemcpyDeviceToHost, h->stream);
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  scratch_free(h, buf);
+  if (e != cudaSuccess) return cuda_fail(h, e, "accel_at");
+  for (uint32_t i = 0; i < nq; ++i) {
+    ax[i] = r[i].x;
+    ay[i] = r[i].y;
+  }
+  return NBX_OK;
 }
 
 // ------------------------------------------------------------ autotuner

@@ -141,24 +141,24 @@ __global__ void __launch_bounds__(kBlock) k_fill_grid(DevState S) {
   }
 }
 
-// Partner discovery.  kFill = false counts, kFill = true writes the lists
-// (small bodies sort their own list in place).
-template <bool kFill>
-__global__ void __launch_bounds__(kBlock) k_partners(DevState S) {
+constexpr uint32_t kStash = 16; // partners remembered per body by the count pass
+
+// Partner discovery, count pass: every overlap of a small body's box in its
+// 3x3 cell neighbourhood and with the large boxes of its instance.  The
+// first kStash partners are stashed so that the fill pass need not search
+// again; small-large pairs are appended for the large body's list.
+__global__ void __launch_bounds__(kBlock) k_partners_count(DevState S) {
   const uint32_t n = S.n;
   const uint32_t mask = S.nBuckets - 1;
-  const uint32_t cap = S.pairCapacity;
-  const bool overflow = kFill && S.counters[0] > cap;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += gridDim.x * blockDim.x) {
     const uint32_t sg = S.segOf[i];
     const float4 bi = S.box[i];
     const uint32_t lStart = S.largeStartA[sg];
     const uint32_t lCount = S.largeCount[sg];
-    const bool iLarge = (S.slot[i] & 0x80000000u) != 0;
     uint32_t cnt = 0;
-    uint32_t base = kFill ? S.pstart[i] : 0u;
-    if (!iLarge) {
+    uint32_t *stash = S.stash + (size_t)i * kStash;
+    if (!(S.slot[i] & 0x80000000u)) {
       const int2 c = S.cellXY[i];
       for (int dy = -1; dy <= 1; ++dy) {
         for (int dx = -1; dx <= 1; ++dx) {
@@ -170,9 +170,8 @@ __global__ void __launch_bounds__(kBlock) k_partners(DevState S) {
             if (j == i) continue;
             const int2 cj = S.cellXY[j];
             if (cj.x != ncx || cj.y != ncy || S.segOf[j] != sg) continue;
-            const float4 bj = S.box[j];
-            if (boxes_overlap(bi, i, bj, j)) {
-              if (kFill && !overflow) S.plist[base + cnt] = j;
+            if (boxes_overlap(bi, i, S.box[j], j)) {
+              if (cnt < kStash) stash[cnt] = j;
               ++cnt;
             }
           }
@@ -180,67 +179,117 @@ __global__ void __launch_bounds__(kBlock) k_partners(DevState S) {
       }
       for (uint32_t k = 0; k < lCount; ++k) {
         const uint32_t j = S.largeList[lStart + k];
-        const float4 bj = S.box[j];
-        if (boxes_overlap(bi, i, bj, j)) {
-          if (kFill) {
-            if (!overflow) {
-              S.plist[base + cnt] = j;
-              const uint32_t slotJ = atomicAdd(&S.fillLarge[j], 1u);
-              S.plist[S.pstart[j] + slotJ] = i;
-            }
-          } else {
-            atomicAdd(&S.deg[j], 1u);
-          }
+        if (boxes_overlap(bi, i, S.box[j], j)) {
+          if (cnt < kStash) stash[cnt] = j;
           ++cnt;
+          atomicAdd(&S.deg[j], 1u);
+          const uint32_t slot = atomicAdd(&S.counters[5], 1u);
+          if (slot < S.n) S.largePairs[slot] = make_uint2(j, i);
+          else atomicOr(S.status, kStatusPairCapacity);
         }
       }
-      if (!kFill) {
-        S.deg[i] = cnt;
-      } else if (overflow) {
-        S.nLater[i] = 0;
-        S.unitFlag[i] = 0;
-        if (i == 0) atomicOr(S.status, kStatusPairCapacity);
-      } else {
-        // insertion sort of the own list by the partners' before() order
-        uint32_t nl = 0;
-        for (uint32_t a = 1; a < cnt; ++a) {
-          const uint32_t v = S.plist[base + a];
-          const float vk = S.box[v].x;
-          uint32_t b = a;
-          while (b > 0) {
-            const uint32_t u = S.plist[base + b - 1];
-            if (!before_key(vk, v, S.box[u].x, u)) break;
-            S.plist[base + b] = u;
-            --b;
-          }
-          S.plist[base + b] = v;
-        }
-        for (uint32_t a = 0; a < cnt; ++a) {
-          const uint32_t u = S.plist[base + a];
-          if (before_key(S.box[u].x, u, bi.x, i)) ++nl;
-        }
-        S.nLater[i] = nl;
-        S.unitFlag[i] = nl > 0 ? 1u : 0u;
-      }
+      S.deg[i] = cnt;
     } else {
-      // large vs large (both directions are visited; each side records
-      // its own half)
+      // large vs large: each side counts its own half
       for (uint32_t k = 0; k < lCount; ++k) {
         const uint32_t j = S.largeList[lStart + k];
-        if (j == i) continue;
-        const float4 bj = S.box[j];
-        if (boxes_overlap(bi, i, bj, j)) {
-          if (kFill) {
-            if (!overflow) {
-              const uint32_t slotI = atomicAdd(&S.fillLarge[i], 1u);
-              S.plist[S.pstart[i] + slotI] = j;
-            }
+        if (j != i && boxes_overlap(bi, i, S.box[j], j)) ++cnt;
+      }
+      atomicAdd(&S.deg[i], cnt);
+    }
+  }
+}
+
+// Fill pass: small bodies copy their stash (or search again past kStash
+// partners) into their CSR list and sort it by the partners' before()
+// order; large bodies add their large-large partners.
+__global__ void __launch_bounds__(kBlock) k_partners_fill(DevState S) {
+  const uint32_t n = S.n;
+  const uint32_t mask = S.nBuckets - 1;
+  const bool overflow = S.counters[0] > S.pairCapacity;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t sg = S.segOf[i];
+    const float4 bi = S.box[i];
+    const uint32_t lStart = S.largeStartA[sg];
+    const uint32_t lCount = S.largeCount[sg];
+    if (S.slot[i] & 0x80000000u) {
+      if (!overflow) {
+        for (uint32_t k = 0; k < lCount; ++k) {
+          const uint32_t j = S.largeList[lStart + k];
+          if (j != i && boxes_overlap(bi, i, S.box[j], j)) {
+            const uint32_t slotI = atomicAdd(&S.fillLarge[i], 1u);
+            S.plist[S.pstart[i] + slotI] = j;
           }
-          ++cnt;
         }
       }
-      if (!kFill) atomicAdd(&S.deg[i], cnt);
+      continue;
     }
+    if (overflow) {
+      S.nLater[i] = 0;
+      S.unitFlag[i] = 0;
+      if (i == 0) atomicOr(S.status, kStatusPairCapacity);
+      continue;
+    }
+    const uint32_t cnt = S.deg[i];
+    const uint32_t base = S.pstart[i];
+    if (cnt <= kStash) {
+      const uint32_t *stash = S.stash + (size_t)i * kStash;
+      for (uint32_t a = 0; a < cnt; ++a) S.plist[base + a] = stash[a];
+    } else {
+      uint32_t w = 0;
+      const int2 c = S.cellXY[i];
+      for (int dy = -1; dy <= 1; ++dy) {
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int ncx = c.x + dx, ncy = c.y + dy;
+          const uint32_t h = cell_hash(sg, ncx, ncy, mask);
+          const uint32_t e0 = S.bucketStart[h], e1 = S.bucketStart[h + 1];
+          for (uint32_t e = e0; e < e1; ++e) {
+            const uint32_t j = S.grid[e];
+            if (j == i) continue;
+            const int2 cj = S.cellXY[j];
+            if (cj.x != ncx || cj.y != ncy || S.segOf[j] != sg) continue;
+            if (boxes_overlap(bi, i, S.box[j], j)) S.plist[base + w++] = j;
+          }
+        }
+      }
+      for (uint32_t k = 0; k < lCount; ++k) {
+        const uint32_t j = S.largeList[lStart + k];
+        if (boxes_overlap(bi, i, S.box[j], j)) S.plist[base + w++] = j;
+      }
+    }
+    // insertion sort of the own list by the partners' before() order
+    for (uint32_t a = 1; a < cnt; ++a) {
+      const uint32_t v = S.plist[base + a];
+      const float vk = S.box[v].x;
+      uint32_t b = a;
+      while (b > 0) {
+        const uint32_t u = S.plist[base + b - 1];
+        if (!before_key(vk, v, S.box[u].x, u)) break;
+        S.plist[base + b] = u;
+        --b;
+      }
+      S.plist[base + b] = v;
+    }
+    uint32_t nl = 0;
+    for (uint32_t a = 0; a < cnt; ++a) {
+      const uint32_t u = S.plist[base + a];
+      if (before_key(S.box[u].x, u, bi.x, i)) ++nl;
+    }
+    S.nLater[i] = nl;
+    S.unitFlag[i] = nl > 0 ? 1u : 0u;
+  }
+}
+
+// Small-large pairs recorded by the count pass, into the large lists.
+__global__ void __launch_bounds__(kBlock) k_fill_large_pairs(DevState S) {
+  if (S.counters[0] > S.pairCapacity) return;
+  const uint32_t total = min(S.counters[5], S.n);
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total;
+       p += gridDim.x * blockDim.x) {
+    const uint2 pr = S.largePairs[p];
+    const uint32_t slot = atomicAdd(&S.fillLarge[pr.x], 1u);
+    S.plist[S.pstart[pr.x] + slot] = pr.y;
   }
 }
 
@@ -402,64 +451,75 @@ __global__ void __launch_bounds__(kBlock) k_twins(DevState S) {
   }
 }
 
-// Ordered resolution.  A warp claims 32 consecutive units (before() order)
-// and loops: every lane whose next pair is ready (body E has completed the
-// chain entries before this pair) resolves it; lanes that are not ready
-// simply try again next round.  No lane ever spins alone, so a lane whose
-// predecessor belongs to another lane of the same warp cannot starve it.
+// Ordered resolution.  Lanes claim units in before() order through one
+// atomic counter (warp-aggregated, so claims stay in order), and every
+// round each lane whose next pair is ready (body E has completed the chain
+// entries before this pair) resolves it; a lane whose unit is done claims
+// the next one.  No lane ever spins alone, so a lane whose predecessor
+// belongs to another lane of the same warp cannot starve it, and the
+// smallest unfinished unit (all its predecessors done) always advances.
 __global__ void __launch_bounds__(kBlock)
     k_resolve(DevState S, const uint32_t *__restrict__ units) {
   const uint32_t numUnits = S.counters[1];
   const int lane = threadIdx.x & 31;
   if (S.counters[0] > S.pairCapacity) return;
+  bool active = false, exhausted = false;
+  uint32_t L = 0, nl = 0, pl = 0, k = 0, E = 0, m = 0;
+  float2 mrL = make_float2(0.0f, 0.0f);
+  float4 sL = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  uint32_t idle = 0;
   for (;;) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(&S.counters[2], 32u);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= numUnits) break;
-    const uint32_t u = base + lane;
-    bool active = u < numUnits;
-    uint32_t L = 0, nl = 0, pl = 0, k = 0, E = 0, m = 0;
-    float2 mrL = make_float2(0.0f, 0.0f);
-    float4 sL = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (active) {
-      L = units[u];
-      S.unitOrder[u] = L; // kept for introspection of the pair order
-      nl = S.nLater[L];
-      pl = S.pstart[L];
-      mrL = S.mr[L];
-      sL = S.pv[L];
-      E = S.plist[pl];
-      m = S.twin[pl];
+    if (!exhausted) {
+      const uint32_t need = __ballot_sync(0xffffffffu, !active);
+      if (need) {
+        const int leader = __ffs(need) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(&S.counters[2], (uint32_t)__popc(need));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (!active) {
+          const uint32_t u = base + __popc(need & lanemask_lt());
+          if (u < numUnits) {
+            L = units[u];
+            S.unitOrder[u] = L; // kept for introspection of the pair order
+            nl = S.nLater[L];
+            pl = S.pstart[L];
+            mrL = S.mr[L];
+            sL = __ldcg(&S.pv[L]);
+            k = 0;
+            E = S.plist[pl];
+            m = S.twin[pl];
+            active = true;
+          }
+        }
+        if (base + (uint32_t)__popc(need) >= numUnits) exhausted = true;
+      }
     }
-    uint32_t idle = 0;
-    while (__any_sync(0xffffffffu, active)) {
-      bool progressed = false;
-      if (active && ld_acquire_u32(&S.prog[E]) == m) {
-        const float2 mrE = S.mr[E];
-        float4 sE = __ldcg(&S.pv[E]);
-        resolve_pair(sL, mrL.x, mrL.y, sE, mrE.x, mrE.y);
-        __stcg(&S.pv[E], sE);
-        st_release_u32(&S.prog[E], m + 1);
-        progressed = true;
-        if (++k == nl) {
-          __stcg(&S.pv[L], sL);
-          st_release_u32(&S.prog[L], nl);
-          active = false;
-        } else {
-          E = S.plist[pl + k];
-          m = S.twin[pl + k];
-        }
-      }
-      if (__any_sync(0xffffffffu, progressed)) {
-        idle = 0;
+    if (!__any_sync(0xffffffffu, active)) break; // nothing left to claim
+    bool progressed = false;
+    if (active && ld_acquire_u32(&S.prog[E]) == m) {
+      const float2 mrE = S.mr[E];
+      float4 sE = __ldcg(&S.pv[E]);
+      resolve_pair(sL, mrL.x, mrL.y, sE, mrE.x, mrE.y);
+      __stcg(&S.pv[E], sE);
+      st_release_u32(&S.prog[E], m + 1);
+      progressed = true;
+      if (++k == nl) {
+        __stcg(&S.pv[L], sL);
+        st_release_u32(&S.prog[L], nl);
+        active = false;
       } else {
-        if (++idle > kSpinLimit) {
-          if (lane == 0) atomicOr(S.status, kStatusSpinLimit);
-          break;
-        }
-        __nanosleep(32);
+        E = S.plist[pl + k];
+        m = S.twin[pl + k];
       }
+    }
+    if (__any_sync(0xffffffffu, progressed)) {
+      idle = 0;
+    } else {
+      if (++idle > kSpinLimit) {
+        if (lane == 0) atomicOr(S.status, kStatusSpinLimit);
+        break;
+      }
+      __nanosleep(32);
     }
   }
 }
@@ -564,12 +624,14 @@ void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
                      scan, S.status);
   k_fill_grid<<<grid_for(n), kBlock, 0, s>>>(S);
   mark(s, "collide.grid");
-  // partners: count, scan, fill + sort
-  k_partners<false><<<grid_for(n), kBlock, 0, s>>>(S);
+  // partners: count (+ stash), scan, fill + sort
+  cudaMemsetAsync(&S.counters[5], 0, sizeof(uint32_t), s);
+  k_partners_count<<<grid_for(n), kBlock, 0, s>>>(S);
   exclusive_scan_u32(s, S.deg, S.pstart, n, nullptr, &S.counters[0], scan,
                      S.status);
   mark(s, "collide.count");
-  k_partners<true><<<grid_for(n), kBlock, 0, s>>>(S);
+  k_partners_fill<<<grid_for(n), kBlock, 0, s>>>(S);
+  k_fill_large_pairs<<<64, kBlock, 0, s>>>(S);
   k_sort_large<<<64, kBlock, 0, s>>>(S);
   mark(s, "collide.fill");
   // units in before() order

@@ -119,7 +119,8 @@ __global__ void __launch_bounds__(kForceBlock)
     k_forces(DevState S, float tSq, float eSq,
              unsigned long long *counts = nullptr,
              const MlpDev *__restrict__ mlp = nullptr, float bandSq = 0.0f,
-             float eps = 0.0f) {
+             float eps = 0.0f, const float2 *__restrict__ query = nullptr,
+             uint32_t nQuery = 0, float2 *__restrict__ queryAcc = nullptr) {
   __shared__ float4 sA[kWarps][32];
   __shared__ int4 sB[kWarps][32];
   __shared__ float4 sBody[kWarps][32];
@@ -134,17 +135,25 @@ __global__ void __launch_bounds__(kForceBlock)
   const int w = threadIdx.x >> 5;
   const uint32_t totalNodes = S.counters[4];
   const uint32_t warpsTotal = (gridDim.x * blockDim.x) >> 5;
+  // query points (instance 0's tree) instead of the bodies, if given
+  const uint32_t nTargets = query ? nQuery : S.n;
   for (uint32_t wb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
-       wb < S.n; wb += warpsTotal * 32) {
+       wb < nTargets; wb += warpsTotal * 32) {
     const uint32_t i = wb + lane;
-    const bool valid = i < S.n;
+    const bool valid = i < nTargets;
     float x = 0.0f, y = 0.0f;
     uint32_t cur = kDone, endNode = 0;
     if (valid) {
-      const float4 b = S.xym[i];
-      x = b.x;
-      y = b.y;
-      const SegDev &G = S.seg[S.segOf[i]];
+      if (query) {
+        const float2 q = query[i];
+        x = q.x;
+        y = q.y;
+      } else {
+        const float4 b = S.xym[i];
+        x = b.x;
+        y = b.y;
+      }
+      const SegDev &G = S.seg[query ? 0u : S.segOf[i]];
       if (G.travCount > 0) {
         cur = G.nodeBase;
         endNode = G.nodeBase + G.travCount;
@@ -268,7 +277,8 @@ __global__ void __launch_bounds__(kForceBlock)
         atomicAdd(&counts[4], (unsigned long long)nTile);
       }
     } else if (valid) {
-      S.acc[i] = make_float2(ax, ay);
+      if (query) queryAcc[i] = make_float2(ax, ay);
+      else S.acc[i] = make_float2(ax, ay);
     }
   }
 }
@@ -323,6 +333,21 @@ double fp32_fma_peak_tflops(cudaStream_t s) {
   cudaFree(out);
   const double flops = 2.0 * 8.0 * (double)iters * blocks * threads;
   return ms > 0 ? flops / (ms * 1e-3) / 1e12 : 0.0;
+}
+
+// Accelerations at arbitrary points from instance 0's last tree
+// (QuadTree::acceleration, QuadTree.cpp:264-389, for any query position).
+void launch_query_forces(cudaStream_t s, const DevState &S, bool exact,
+                         const float2 *query, uint32_t nq, float2 *out) {
+  const uint32_t b = ((nq + 31) / 32 + kWarps - 1) / kWarps;
+  if (exact)
+    k_forces<true><<<b ? b : 1, kForceBlock, 0, s>>>(S, S.tSq, S.eSq, nullptr,
+                                                     nullptr, 0.0f, 0.0f, query,
+                                                     nq, out);
+  else
+    k_forces<false><<<b ? b : 1, kForceBlock, 0, s>>>(S, S.tSq, S.eSq, nullptr,
+                                                      nullptr, 0.0f, 0.0f, query,
+                                                      nq, out);
 }
 
 void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,

@@ -69,6 +69,8 @@ struct DevState {
   uint32_t *plist;       // partner indices
   uint32_t *plistTmp;    // scratch copy used to sort large bodies' lists
   uint32_t *twin;        // per as-later entry: position in the partner's list
+  uint32_t *stash;       // first partners of each body found by the count pass
+  uint2 *largePairs;     // (large, small) pairs found by the count pass
   uint32_t *fillLarge;   // fill counters of large bodies
   uint32_t *nLater;      // partners that sort before the body
   uint32_t *unitFlag;    // nLater > 0
@@ -77,6 +79,7 @@ struct DevState {
   uint32_t *unitOrder;   // units in before() order (last collide)
   uint32_t *counters;    // [0]=pairs*2 total [1]=units [2]=unit claim
                          // [3]=splitting entries [4]=total nodes
+                         // [5]=small-large pairs [8]=id check
 
   // Morton / sort
   uint64_t *codes; // unsorted codes (kept for the segment passes)

@@ -75,3 +75,50 @@ def test_create_without_device_reports_error(nbx):
                          text=True, env=env, timeout=120)
     assert out.returncode == 0, out.stderr
     assert out.stdout.startswith("error"), out.stdout
+
+
+def read_nbs2(path):
+    """Reads an NBS2 file (layout of the reference's Main.cpp:13-49)."""
+    raw = open(path, "rb").read()
+    hdr = np.frombuffer(raw[:28], np.dtype([
+        ("magic", "S4"), ("n", "<u4"), ("steps", "<u4"), ("every", "<u4"),
+        ("frames", "<u4"), ("completed", "<u4"), ("dt", "<f4")]))[0]
+    n = int(hdr["n"])
+    mass = np.frombuffer(raw[28:28 + 4 * n], "<f4")
+    radius = np.frombuffer(raw[28 + 4 * n:28 + 8 * n], "<f4")
+    body = raw[28 + 8 * n:]
+    k = len(body) // (16 * n) if n else 0
+    frames = np.frombuffer(body[:16 * n * k], "<f4").reshape(k, n, 4)
+    return hdr, mass, radius, frames
+
+
+def test_nbs2_writer(nbx, tmp_path):
+    import ctypes as C
+    L = nbx.lib()
+    L.nbx_nbs2_open.argtypes = [C.c_char_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                C.c_float, C.c_void_p, C.c_void_p,
+                                C.POINTER(C.c_void_p)]
+    L.nbx_nbs2_write_frame.argtypes = [C.c_void_p, C.c_void_p]
+    L.nbx_nbs2_close.argtypes = [C.c_void_p]
+    b = nbx.uniform_disc(300)
+    b = np.sort(b, order="id")
+    path = str(tmp_path / "t.bin")
+    w = C.c_void_p()
+    assert L.nbx_nbs2_open(path.encode(), 300, 20, 10, 0.05,
+                           np.ascontiguousarray(b["mass"]).ctypes.data,
+                           np.ascontiguousarray(b["radius"]).ctypes.data,
+                           C.byref(w)) == 0
+    written = []
+    for k in range(2):
+        assert L.nbx_nbs2_write_frame(w, b.ctypes.data) == 0
+        written.append(b.copy())
+        hdr, _, _, frames = read_nbs2(path)
+        assert hdr["completed"] == k + 1 and len(frames) == k + 1  # live counter
+        b["px"] += 1.0
+    assert L.nbx_nbs2_close(w) == 0
+    hdr, mass, radius, frames = read_nbs2(path)
+    assert hdr["magic"] == b"NBS2" and hdr["n"] == 300 and hdr["frames"] == 3
+    assert hdr["completed"] == 2 and np.float32(hdr["dt"]) == np.float32(0.05)
+    assert np.array_equal(mass, b["mass"]) and np.array_equal(radius, b["radius"])
+    assert np.array_equal(frames[1][:, 0], written[1]["px"])
+    assert np.array_equal(frames[0][:, 2], written[0]["vx"])
