@@ -31,15 +31,24 @@ namespace {
 
 constexpr int kBlock = 256;
 
+// Bucket of a grid cell: the Morton interleave of the cell coordinates
+// (low 16 bits of each), so that cells close in space -- and bodies close in
+// the current, Morton-sorted, array order -- share cache lines of the
+// bucket table; instances are offset by a large odd stride.  Distinct cells
+// may share a bucket; lookups filter on the exact cell.
 __device__ __forceinline__ uint32_t cell_hash(uint32_t seg, int cx, int cy,
                                               uint32_t mask) {
-  uint32_t h = (uint32_t)cx * 0x9E3779B1u;
-  h ^= (uint32_t)cy * 0x85EBCA77u + (h << 6) + (h >> 2);
-  h ^= seg * 0xC2B2AE3Du;
-  h ^= h >> 15;
-  h *= 0x2C1B3C6Du;
-  h ^= h >> 13;
-  return h & mask;
+  uint32_t x = (uint32_t)cx & 0xffffu, y = (uint32_t)cy & 0xffffu;
+  x = (x | (x << 8)) & 0x00FF00FFu;
+  x = (x | (x << 4)) & 0x0F0F0F0Fu;
+  x = (x | (x << 2)) & 0x33333333u;
+  x = (x | (x << 1)) & 0x55555555u;
+  y = (y | (y << 8)) & 0x00FF00FFu;
+  y = (y | (y << 4)) & 0x0F0F0F0Fu;
+  y = (y | (y << 2)) & 0x33333333u;
+  y = (y | (y << 1)) & 0x55555555u;
+  const uint32_t hi = ((uint32_t)cx >> 16) * 0x9E3779B1u ^ ((uint32_t)cy >> 16) * 0x85EBCA77u;
+  return ((x | (y << 1)) + hi + seg * 0x2545F491u) & mask;
 }
 
 // floor of the exact product v*inv (the reference takes the floor of the

@@ -6,6 +6,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from conftest import ROOT, same_bits
 
@@ -36,6 +37,14 @@ def test_params_default_are_reference_defaults(nbx):
     p = nbx.default_params()
     assert (p.dt, p.theta, p.epsilon, p.leaf_capacity, p.collisions) == (
         np.float32(0.05), 1.0, 1.0, 16, 1)
+
+
+@pytest.mark.parametrize("bad", [dict(use_mlp=3), dict(leaf_capacity=0),
+                                 dict(leaf_capacity=65), dict(theta=-1.0)])
+def test_invalid_params_rejected_before_device(nbx, bad):
+    with pytest.raises(nbx.NbxError) as e:
+        nbx.Handle([16], **bad)
+    assert e.value.code == 1  # NBX_ERR_ARG
 
 
 def test_two_discs_layout(nbx):
