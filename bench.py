@@ -317,6 +317,9 @@ def run_b200(args):
     sim.step(args.warmup)
     sim.sync()
     kernels_per_step = sim.step_kernels()
+    # state at the start of the timed region: a second handle replays the
+    # timed steps afterwards to count each step's interactions
+    start_state = sim.download()
 
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -325,7 +328,8 @@ def run_b200(args):
         torch.cuda.synchronize(local)
         sim.sync()
         e0.record(stream)
-        sim.step(args.steps)
+        # the step graph with CUDA events around each force launch
+        sim.step_timed(args.steps)
         e1.record(stream)
         e1.synchronize()
         sim.sync()
@@ -335,24 +339,29 @@ def run_b200(args):
     ms = max_over_ranks(dist, local, ms_rank)
     value = world * n / (ms * 1e-3)
 
-    # dominant kernel: the force traversal, timed alone on the same stream
-    inter = sim.interactions()
-    reps = 5
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    sim.phase("forces")
-    f0.record(stream)
-    for _ in range(reps):
-        sim.phase("forces")
-    f1.record(stream)
-    f1.synchronize()
-    force_ms = f0.elapsed_time(f1) / reps
+    # dominant kernel: the force traversal.  Its per-step durations were
+    # recorded inside the timed region; its work per step comes from a
+    # replay of the same steps on a second handle, which counts each
+    # step's interactions (the simulation is deterministic: the replay's
+    # final state must equal the timed run's bit for bit).
+    force_ms_steps = sim.force_times(args.steps)
+    s = sim.download()
+    replay = nbx.Simulation(start_state, theta=THETA, device=local)
+    inter_steps = np.empty((args.steps, 2), np.float64)
+    for k in range(args.steps):
+        replay.step(1)
+        c = replay.interactions()
+        inter_steps[k] = c["far"], c["near"]
+    replay_same = replay.download().tobytes() == s.tobytes()
+    replay.close()
+    inter = {"far": inter_steps[:, 0].mean(), "near": inter_steps[:, 1].mean()}
+    force_ms = float(force_ms_steps.mean())
     flops = FLOP_PER_INTERACTION * (inter["far"] + inter["near"])
-    achieved = flops / (force_ms * 1e-3) / 1e12
+    achieved = (FLOP_PER_INTERACTION * inter_steps.sum()
+                / (force_ms_steps.astype(np.float64).sum() * 1e-3) / 1e12)
     peak = nbx.fp32_peak_tflops()
 
     # force error against the FP64 direct sum on 4096 sampled bodies
-    s = sim.download()
     rng = np.random.default_rng(12345)
     ids = rng.choice(n, 4096, replace=False)
     pos = np.empty(n, np.int64)
@@ -418,7 +427,14 @@ def run_b200(args):
             "peak_note": "FP32 FMA peak measured live by a probe kernel "
                          "(MEASURED_PEAKS.json holds no FP32 figure)",
             "flops_per_launch": flops, "launch_ms": force_ms,
+            "launch_ms_first_last": [float(force_ms_steps[0]), float(force_ms_steps[-1])],
+            "force_share_of_step": force_ms / ms,
             "interactions_per_body": (inter["far"] + inter["near"]) / n,
+            "timing": "CUDA events around every force launch of the timed "
+                      "steps (event-record nodes in the step graph, same stream); "
+                      "FLOPs from a replay of the same steps counting "
+                      "interactions per step",
+            "replay_bit_identical": replay_same,
         },
         "force_error_fp64": {"p50": err_stats["median"], "p99": err_stats["p99"],
                              "max": err_stats["max"], "samples": 4096},

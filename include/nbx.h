@@ -123,6 +123,16 @@ int nbx_download_bodies(nbx_handle *h, nbx_body *bodies, size_t n,
  * per step and returns; errors raised on the device surface at nbx_sync. */
 int nbx_step(nbx_handle *h, uint32_t steps);
 
+/* nbx_step with the duration of each step's force pass recorded by CUDA
+ * events on the handle's stream, around the force launch inside the step's
+ * graph (the same kernels as nbx_step, plus two event records per step).
+ * Asynchronous like nbx_step; nbx_force_times synchronises and returns the
+ * first `count` per-step durations (ms) of the last nbx_step_timed call.
+ * No counterpart in the reference, which times whole sim.step() calls
+ * only (src/Main.cpp:172-180). */
+int nbx_step_timed(nbx_handle *h, uint32_t steps);
+int nbx_force_times(nbx_handle *h, float *ms, uint32_t count);
+
 /* Waits for the handle's stream and reports (and clears) device-side
  * error bits: NBX_ERR_CAPACITY, NBX_ERR_NONFINITE, NBX_ERR_TIMEOUT. */
 int nbx_sync(nbx_handle *h);

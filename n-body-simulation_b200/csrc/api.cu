@@ -133,6 +133,16 @@ struct nbx_handle {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   uint32_t graphKernels = 0; // kernel nodes per captured step
   bool graphsValid = false;
+  // timed step graphs: the same step with event-record nodes around the
+  // force launch; each launch points them at the next pair of pool events
+  cudaGraph_t graphTSrc[2] = {nullptr, nullptr};
+  cudaGraphExec_t graphT[2] = {nullptr, nullptr};
+  cudaGraphNode_t forceEvNode[2][2] = {};
+  cudaEvent_t forceMark[2] = {nullptr, nullptr}; // placeholders at capture
+  std::vector<cudaEvent_t> forceEv;               // 2 per timed step
+  uint32_t timedSteps = 0;                        // steps of the last call
+  bool timedValid = false;
+  bool timedCapture = false;
   bool uploaded = false;
   bool treeValid = false;
   bool collideValid = false;
@@ -208,7 +218,8 @@ int allocate(nbx_handle *h) {
   const double nf = P.node_factor > 0 ? P.node_factor : 8.0f;
   S.nodeCapacity = (uint32_t)std::min<double>(nf * n + 8.0 * ns + 8, 2.0e9);
   const double pf = P.pair_factor > 0 ? P.pair_factor : 32.0f;
-  S.pairCapacity = (uint32_t)std::min<double>(pf * n + 64, 2.0e9);
+  // chain entry indices carry two flag bits (collide.cu): below 2^30
+  S.pairCapacity = (uint32_t)std::min<double>(pf * n + 64, (double)(1u << 30) - 64.0);
   S.nBuckets = next_pow2(2ull * std::max<uint32_t>(n, 1));
   const uint32_t nodes = S.nodeCapacity;
   const uint32_t sortCap = 2 * n + 64;
@@ -246,7 +257,7 @@ int allocate(nbx_handle *h) {
   A(S.nLater, n);
   A(S.unitFlag, n);
   A(S.unitPos, n + 1);
-  A(S.prog, n);
+  A(S.chain, S.pairCapacity);
   A(S.unitOrder, n);
   A(S.counters, 16);
   A(S.codes, n);
@@ -352,9 +363,11 @@ DevState enqueue_step(nbx_handle *h, cudaStream_t s, DevState S) {
   mark(s, "integrate");
   if (S.collisions) launch_collide(s, S, h->scan, h->sort);
   launch_build(s, S, h->scan, h->sort);
+  if (h->timedCapture) cudaEventRecordWithFlags(h->forceMark[0], s, cudaEventRecordExternal);
   launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
                 h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
                 h->params.use_mlp);
+  if (h->timedCapture) cudaEventRecordWithFlags(h->forceMark[1], s, cudaEventRecordExternal);
   mark(s, "forces");
   return S;
 }
@@ -365,6 +378,58 @@ void destroy_graphs(nbx_handle *h) {
     g = nullptr;
   }
   h->graphsValid = false;
+  for (int p = 0; p < 2; ++p) {
+    if (h->graphT[p]) cudaGraphExecDestroy(h->graphT[p]);
+    if (h->graphTSrc[p]) cudaGraphDestroy(h->graphTSrc[p]);
+    h->graphT[p] = nullptr;
+    h->graphTSrc[p] = nullptr;
+  }
+  h->timedValid = false;
+}
+
+// Step graphs with the force launch bracketed by event-record nodes (kept
+// with their source graphs, whose node handles re-point the events).
+int capture_timed_graphs(nbx_handle *h) {
+  for (int q = 0; q < 2; ++q)
+    if (!h->forceMark[q]) NBX_CUDA(h, cudaEventCreate(&h->forceMark[q]));
+  for (int p = 0; p < 2; ++p) {
+    if (h->graphT[p]) cudaGraphExecDestroy(h->graphT[p]);
+    if (h->graphTSrc[p]) cudaGraphDestroy(h->graphTSrc[p]);
+    h->graphT[p] = nullptr;
+    h->graphTSrc[p] = nullptr;
+    const int saved = h->cur;
+    h->cur = p;
+    const DevState S = h->state();
+    h->cur = saved;
+    cudaGraph_t g = nullptr;
+    NBX_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    h->timedCapture = true;
+    enqueue_step(h, h->stream, S);
+    h->timedCapture = false;
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+    h->graphTSrc[p] = g;
+    size_t count = 0;
+    cudaGraphGetNodes(g, nullptr, &count);
+    std::vector<cudaGraphNode_t> nodes(count);
+    cudaGraphGetNodes(g, nodes.data(), &count);
+    h->forceEvNode[p][0] = h->forceEvNode[p][1] = nullptr;
+    for (auto nd : nodes) {
+      cudaGraphNodeType t;
+      if (cudaGraphNodeGetType(nd, &t) != cudaSuccess || t != cudaGraphNodeTypeEventRecord)
+        continue;
+      cudaEvent_t ev = nullptr;
+      cudaGraphEventRecordNodeGetEvent(nd, &ev);
+      for (int q = 0; q < 2; ++q)
+        if (ev == h->forceMark[q]) h->forceEvNode[p][q] = nd;
+    }
+    if (!h->forceEvNode[p][0] || !h->forceEvNode[p][1])
+      return fail(h, NBX_ERR_CUDA, "timed step graph lacks its event-record nodes");
+    e = cudaGraphInstantiate(&h->graphT[p], g, 0);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+  }
+  h->timedValid = true;
+  return NBX_OK;
 }
 
 int capture_graphs(nbx_handle *h) {
@@ -488,6 +553,9 @@ int nbx_destroy(nbx_handle *h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   destroy_graphs(h);
+  for (cudaEvent_t ev : h->forceEv) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : h->forceMark)
+    if (ev) cudaEventDestroy(ev);
   for (void *v : h->allocs) cudaFree(v);
   for (void *v : h->scratch) cudaFree(v);
   if (h->hPinned) cudaFreeHost(h->hPinned);
@@ -629,6 +697,50 @@ int nbx_step(nbx_handle *h, uint32_t steps) {
   h->treeValid = true;
   h->collideValid = h->params.collisions != 0;
   return NBX_OK;
+}
+
+int nbx_step_timed(nbx_handle *h, uint32_t steps) {
+  if (!h) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!h->uploaded) return fail(h, NBX_ERR_STATE, "no bodies uploaded");
+  h->timedSteps = 0;
+  if (h->n == 0 || steps == 0) return NBX_OK;
+  if (h->params.use_mlp == 1 && !h->mlpLoaded)
+    return fail(h, NBX_ERR_STATE, "use_mlp = 1 without MLP parameters");
+  if (!h->timedValid) {
+    int rc = capture_timed_graphs(h);
+    if (rc != NBX_OK) return rc;
+  }
+  while (h->forceEv.size() < 2 * (size_t)steps) {
+    cudaEvent_t ev = nullptr;
+    NBX_CUDA(h, cudaEventCreate(&ev));
+    h->forceEv.push_back(ev);
+  }
+  for (uint32_t k = 0; k < steps; ++k) {
+    const int p = h->cur;
+    // affects this and later launches only; earlier launches keep theirs
+    NBX_CUDA(h, cudaGraphExecEventRecordNodeSetEvent(h->graphT[p], h->forceEvNode[p][0],
+                                                     h->forceEv[2 * k]));
+    NBX_CUDA(h, cudaGraphExecEventRecordNodeSetEvent(h->graphT[p], h->forceEvNode[p][1],
+                                                     h->forceEv[2 * k + 1]));
+    NBX_CUDA(h, cudaGraphLaunch(h->graphT[p], h->stream));
+    h->cur ^= 1;
+  }
+  h->timedSteps = steps;
+  h->treeValid = true;
+  h->collideValid = h->params.collisions != 0;
+  return NBX_OK;
+}
+
+int nbx_force_times(nbx_handle *h, float *ms, uint32_t count) {
+  if (!h || (!ms && count)) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (count > h->timedSteps)
+    return fail(h, NBX_ERR_ARG, "more force times requested than steps timed");
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (uint32_t k = 0; k < count; ++k)
+    NBX_CUDA(h, cudaEventElapsedTime(&ms[k], h->forceEv[2 * k], h->forceEv[2 * k + 1]));
+  return check_status(h);
 }
 
 int nbx_sync(nbx_handle *h) {

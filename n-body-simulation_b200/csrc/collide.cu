@@ -21,7 +21,15 @@
 //    entries of its chain that precede L.  Units only ever wait on
 //    smaller units, so the smallest unfinished unit always progresses.
 //    The result equals the sequential loop bit for bit (the resolve
-//    arithmetic below is IEEE op for op, no contraction).
+//    arithmetic below is IEEE op for op, no contraction);
+//  * a body's state after chain entry e is published once, into chain[e]
+//    (16 bytes, preset to a sentinel in every word).  The pair that needs
+//    it polls that record itself: the load that finds no sentinel word
+//    already holds the state, so a dependency costs one L2 round trip and
+//    the producer needs no fence.  A body's final state goes to pv.  A
+//    sentinel word can only be a NaN with every payload bit set (0xffffffff),
+//    which arithmetic never produces; a body carrying one in its input
+//    state makes its consumer's wait run out (status: timeout).
 #include "nbx_state.cuh"
 
 #include <float.h>
@@ -446,35 +454,57 @@ __device__ __forceinline__ uint32_t chain_position(const DevState &S,
   return lo;
 }
 
-// Chain position of each as-later pair (L, E): where L sits in E's sorted
-// partner list.  Computed in bulk so the resolution does not search.
+constexpr uint32_t kUnpublished = 0xffffffffu; // sentinel word of chain[]
+constexpr uint32_t kFirstEntry = 1u << 31;      // E's chain starts here
+constexpr uint32_t kLastEntry = 1u << 30;       // E's chain ends here
+constexpr uint32_t kEntryMask = kLastEntry - 1u;
+
+__device__ __forceinline__ bool published(const float4 &v) {
+  return (__float_as_uint(v.x) != kUnpublished) & (__float_as_uint(v.y) != kUnpublished) &
+         (__float_as_uint(v.z) != kUnpublished) & (__float_as_uint(v.w) != kUnpublished);
+}
+
+// Per as-later pair (L, E): E's chain entry for it (where L sits in E's
+// sorted partner list, offset by E's list start), flagged when it is E's
+// first or last entry; computed in bulk so the resolution does not search.
+// Also presets every chain record of the body to the sentinel.
 __global__ void __launch_bounds__(kBlock) k_twins(DevState S) {
+  if (S.counters[0] > S.pairCapacity) return;
+  const float4 unset = make_float4(__uint_as_float(kUnpublished), __uint_as_float(kUnpublished),
+                                   __uint_as_float(kUnpublished), __uint_as_float(kUnpublished));
   for (uint32_t L = blockIdx.x * blockDim.x + threadIdx.x; L < S.n;
        L += gridDim.x * blockDim.x) {
+    const uint32_t pl = S.pstart[L], dl = S.deg[L];
+    for (uint32_t k = 0; k < dl; ++k) __stcg(&S.chain[pl + k], unset);
     const uint32_t nl = S.nLater[L];
-    if (!nl) continue;
-    const uint32_t pl = S.pstart[L];
     const float key = S.box[L].x;
-    for (uint32_t k = 0; k < nl; ++k)
-      S.twin[pl + k] = chain_position(S, S.plist[pl + k], L, key);
+    for (uint32_t k = 0; k < nl; ++k) {
+      const uint32_t E = S.plist[pl + k];
+      const uint32_t m = chain_position(S, E, L, key);
+      S.twin[pl + k] = (S.pstart[E] + m) | (m == 0 ? kFirstEntry : 0u) |
+                       (m + 1 == S.deg[E] ? kLastEntry : 0u);
+    }
   }
 }
 
 // Ordered resolution.  Lanes claim units in before() order through one
 // atomic counter (warp-aggregated, so claims stay in order), and every
-// round each lane whose next pair is ready (body E has completed the chain
-// entries before this pair) resolves it; a lane whose unit is done claims
-// the next one.  No lane ever spins alone, so a lane whose predecessor
-// belongs to another lane of the same warp cannot starve it, and the
-// smallest unfinished unit (all its predecessors done) always advances.
+// round each lane whose next pair is ready (body E's state after the chain
+// entries before this pair is published) resolves it; a lane whose unit is
+// done claims the next one.  No lane ever spins alone, so a lane whose
+// predecessor belongs to another lane of the same warp cannot starve it,
+// and the smallest unfinished unit (all its predecessors done) always
+// advances.  The next pair's partner is fetched while the current one waits.
 __global__ void __launch_bounds__(kBlock)
     k_resolve(DevState S, const uint32_t *__restrict__ units) {
   const uint32_t numUnits = S.counters[1];
   const int lane = threadIdx.x & 31;
   if (S.counters[0] > S.pairCapacity) return;
-  bool active = false, exhausted = false;
-  uint32_t L = 0, nl = 0, pl = 0, k = 0, E = 0, m = 0;
-  float2 mrL = make_float2(0.0f, 0.0f);
+  bool active = false, exhausted = false, lastL = false;
+  uint32_t L = 0, nl = 0, pl = 0, k = 0;
+  uint32_t E = 0, t = 0, nE = 0, nt = 0; // current and next pair
+  float2 mrL = make_float2(0.0f, 0.0f), mrE = mrL, nmrE = mrL;
+  bool nmrPending = false;
   float4 sL = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   uint32_t idle = 0;
   for (;;) {
@@ -492,11 +522,18 @@ __global__ void __launch_bounds__(kBlock)
             S.unitOrder[u] = L; // kept for introspection of the pair order
             nl = S.nLater[L];
             pl = S.pstart[L];
+            lastL = nl == S.deg[L];
             mrL = S.mr[L];
             sL = __ldcg(&S.pv[L]);
             k = 0;
             E = S.plist[pl];
-            m = S.twin[pl];
+            t = S.twin[pl];
+            mrE = S.mr[E];
+            if (nl > 1) {
+              nE = S.plist[pl + 1];
+              nt = S.twin[pl + 1];
+              nmrPending = true;
+            }
             active = true;
           }
         }
@@ -505,20 +542,34 @@ __global__ void __launch_bounds__(kBlock)
     }
     if (!__any_sync(0xffffffffu, active)) break; // nothing left to claim
     bool progressed = false;
-    if (active && ld_acquire_u32(&S.prog[E]) == m) {
-      const float2 mrE = S.mr[E];
-      float4 sE = __ldcg(&S.pv[E]);
-      resolve_pair(sL, mrL.x, mrL.y, sE, mrE.x, mrE.y);
-      __stcg(&S.pv[E], sE);
-      st_release_u32(&S.prog[E], m + 1);
-      progressed = true;
-      if (++k == nl) {
-        __stcg(&S.pv[L], sL);
-        st_release_u32(&S.prog[L], nl);
-        active = false;
-      } else {
-        E = S.plist[pl + k];
-        m = S.twin[pl + k];
+    if (active) {
+      if (nmrPending) { // nE has arrived by now
+        nmrE = S.mr[nE];
+        nmrPending = false;
+      }
+      const uint32_t e = t & kEntryMask;
+      const bool first = (t & kFirstEntry) != 0;
+      float4 sE = first ? __ldcg(&S.pv[E]) : ld_relaxed_f4(&S.chain[e - 1]);
+      if (first || published(sE)) {
+        resolve_pair(sL, mrL.x, mrL.y, sE, mrE.x, mrE.y);
+        if (t & kLastEntry) __stcg(&S.pv[E], sE);
+        else st_relaxed_f4(&S.chain[e], sE);
+        progressed = true;
+        if (++k == nl) {
+          // L's own entries are the first of its chain: publish its state
+          if (lastL) __stcg(&S.pv[L], sL);
+          else st_relaxed_f4(&S.chain[pl + nl - 1], sL);
+          active = false;
+        } else {
+          E = nE;
+          t = nt;
+          mrE = nmrE;
+          if (k + 1 < nl) {
+            nE = S.plist[pl + k + 1];
+            nt = S.twin[pl + k + 1];
+            nmrPending = true;
+          }
+        }
       }
     }
     if (__any_sync(0xffffffffu, progressed)) {
@@ -651,7 +702,6 @@ void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
                                  false, S.status);
   mark(s, "collide.units");
   // ordered resolution
-  cudaMemsetAsync(S.prog, 0, sizeof(uint32_t) * n, s);
   cudaMemsetAsync(&S.counters[2], 0, sizeof(uint32_t), s);
   k_twins<<<grid_for(n), kBlock, 0, s>>>(S);
   k_resolve<<<148 * 8, kBlock, 0, s>>>(S, sort.vals[buf]);

@@ -68,14 +68,16 @@ struct DevState {
   uint32_t *pstart;      // CSR start per body
   uint32_t *plist;       // partner indices
   uint32_t *plistTmp;    // scratch copy used to sort large bodies' lists
-  uint32_t *twin;        // per as-later entry: position in the partner's list
+  uint32_t *twin;        // per as-later entry: the partner's chain entry
+                         // (index | kFirstEntry | kLastEntry)
+  float4 *chain;         // per chain entry: the body's state after it
+                         // (published entries only; sentinel until then)
   uint32_t *stash;       // first partners of each body found by the count pass
   uint2 *largePairs;     // (large, small) pairs found by the count pass
   uint32_t *fillLarge;   // fill counters of large bodies
   uint32_t *nLater;      // partners that sort before the body
   uint32_t *unitFlag;    // nLater > 0
   uint32_t *unitPos;     // scan of unitFlag
-  uint32_t *prog;        // resolved chain entries per body
   uint32_t *unitOrder;   // units in before() order (last collide)
   uint32_t *counters;    // [0]=pairs*2 total [1]=units [2]=unit claim
                          // [3]=splitting entries [4]=total nodes

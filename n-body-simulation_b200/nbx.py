@@ -36,7 +36,7 @@ EXPORTS = (
     "nbx_fp32_peak_tflops", "nbx_profile_step", "nbx_mlp_set_params",
     "nbx_mlp_get_params", "nbx_mlp_init", "nbx_mlp_harvest", "nbx_mlp_train",
     "nbx_mlp_gradient", "nbx_mlp_eval", "nbx_ensemble_sizes", "nbx_autotune",
-    "nbx_direct_fp64_noalloc",
+    "nbx_direct_fp64_noalloc", "nbx_step_timed", "nbx_force_times",
 )
 MLP_PARAMS = 1442
 MLP_ROW = 12
@@ -90,6 +90,8 @@ def lib() -> C.CDLL:
         "nbx_upload_bodies": [vp, vp, C.c_size_t],
         "nbx_download_bodies": [vp, vp, C.c_size_t, C.c_int],
         "nbx_step": [vp, C.c_uint32],
+        "nbx_step_timed": [vp, C.c_uint32],
+        "nbx_force_times": [vp, vp, C.c_uint32],
         "nbx_sync": [vp],
         "nbx_phase": [vp, C.c_int],
         "nbx_get_morton": [vp, C.c_uint32, u64p, u32p, C.c_size_t],
@@ -249,6 +251,16 @@ class Handle:
 
     def step(self, steps: int = 1):
         self._c(lib().nbx_step(self.h, steps))
+
+    def step_timed(self, steps: int):
+        """Like step(), recording each step's force-pass duration on the
+        handle's stream (read them with force_times())."""
+        self._c(lib().nbx_step_timed(self.h, steps))
+
+    def force_times(self, count: int) -> np.ndarray:
+        out = np.empty(count, np.float32)
+        self._c(lib().nbx_force_times(self.h, out.ctypes.data, count))
+        return out
 
     def sync(self):
         self._c(lib().nbx_sync(self.h))

@@ -188,6 +188,29 @@ def test_ten_step_trajectories(nbx, oracle, golden, theta):
     sim.close()
 
 
+def test_step_timed_same_state(nbx):
+    """The timed step graph (event records around the force launch) gives
+    the same trajectory as the plain one and one duration per step."""
+    b = nbx.two_discs(65536, 0, 0.2)
+    a = nbx.Simulation(b, theta=0.5)
+    a.step(7)
+    ra = a.download()
+    a.close()
+    t = nbx.Simulation(b, theta=0.5)
+    t.step_timed(4)
+    t.step(1)
+    t.step_timed(2)
+    ms = t.force_times(2)
+    assert ms.shape == (2,) and (ms > 0).all() and (ms < 1e3).all()
+    assert same_bits(t.download(), ra)
+    with pytest.raises(nbx.NbxError):
+        t.force_times(3)  # only 2 steps in the last timed call
+    t.set_params(theta=0.7)  # new graphs; timing still works
+    t.step_timed(3)
+    assert (t.force_times(3) > 0).all()
+    t.close()
+
+
 def test_deterministic(nbx):
     b = nbx.uniform_disc(20000)
     outs = []
