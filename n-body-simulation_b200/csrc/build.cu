@@ -490,7 +490,10 @@ __global__ void __launch_bounds__(kBlock) k_preorder(DevState S) {
     const uint32_t pg = nb + pre;
     const float sz = S.size[g];
     S.tA[pg] = make_float4(S.comX[g], S.comY[g], S.mass[g], __fmul_rn(sz, sz));
-    S.tB[pg] = make_int4((int)(pg + S.subtree[g]), (int)(G.start + S.start[g]),
+    // next node after this subtree; all ones past the instance's last node
+    const uint32_t skip = pg + S.subtree[g];
+    const uint32_t nextPg = skip >= nb + S.subtree[nb] ? 0xffffffffu : skip;
+    S.tB[pg] = make_int4((int)nextPg, (int)(G.start + S.start[g]),
                          (int)(G.start + S.end[g]), S.children[g] == 0 ? 1 : 0);
     const float4 mo = S.moments[g];
     S.tM[pg] = make_float4(mo.x, mo.y, mo.z, sz);

@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(kForceBlock)
     const uint32_t i = wb + lane;
     const bool valid = i < nTargets;
     float x = 0.0f, y = 0.0f;
-    uint32_t cur = kDone, endNode = 0;
+    uint32_t cur = kDone;
     if (valid) {
       if (query) {
         const float2 q = query[i];
@@ -154,10 +154,7 @@ __global__ void __launch_bounds__(kForceBlock)
         y = b.y;
       }
       const SegDev &G = S.seg[query ? 0u : S.segOf[i]];
-      if (G.travCount > 0) {
-        cur = G.nodeBase;
-        endNode = G.nodeBase + G.travCount;
-      }
+      if (G.travCount > 0) cur = G.nodeBase;
     }
     float ax = 0.0f, ay = 0.0f;
     uint32_t nFar = 0, nNear = 0, nVisit = 0, nIter = 0, nTile = 0;
@@ -179,7 +176,8 @@ __global__ void __launch_bounds__(kForceBlock)
       }
       const float4 A = sA[w][k - tileBase];
       const int4 B = sB[w][k - tileBase];
-      const uint32_t nxt = (uint32_t)B.x > k ? (uint32_t)B.x : kDone;
+      // the node after k's subtree (kDone past the instance's last node)
+      const uint32_t nxt = (uint32_t)B.x;
       // every lane evaluates the node; only the lanes waiting at it use it
       const bool at = cur == k;
       const float dx = kExact ? __fsub_rn(A.x, x) : A.x - x;
@@ -236,7 +234,8 @@ __global__ void __launch_bounds__(kForceBlock)
         if (kCount) nFar += use ? 1u : 0u;
       }
       if (kCount) nVisit += at ? 1u : 0u;
-      cur = accept ? nxt : ((at && !openLeaf) ? k + 1 : cur);
+      // accepted or leaf: skip the subtree; interior node: descend
+      cur = (accept || openLeaf) ? nxt : (at ? k + 1 : cur);
       const uint32_t leafLanes = __ballot_sync(0xffffffffu, openLeaf);
       if (leafLanes) {
         const uint32_t b0 = (uint32_t)B.y, b1 = (uint32_t)B.z;
@@ -258,9 +257,7 @@ __global__ void __launch_bounds__(kForceBlock)
           }
         }
         if (kCount && openLeaf) nNear += bEnd > b0 ? bEnd - b0 : 0u;
-        cur = openLeaf ? nxt : cur;
       }
-      cur = cur >= endNode ? kDone : cur;
     }
     if (kCount) {
       unsigned long long f = nFar, nn = nNear, v = nVisit;

@@ -78,31 +78,41 @@ __global__ void __launch_bounds__(kScanThreads)
     }
     const uint32_t blockTotal = __shfl_sync(0xffffffffu, wi, kScanThreads / 32 - 1);
     if (lane < kScanThreads / 32) s_warp[lane] = wi - w; // exclusive
-    if (lane == 0) {
-      uint64_t excl = 0;
-      if (tile == 0) {
-        st_relaxed_u64(&status[0], kFlagIncl | (uint64_t)blockTotal);
-      } else {
-        st_relaxed_u64(&status[tile], kFlagAgg | (uint64_t)blockTotal);
-        int64_t pred = (int64_t)tile - 1;
-        uint32_t spins = 0;
-        while (pred >= 0) {
-          const uint64_t s = ld_relaxed_u64(&status[pred]);
-          const uint64_t flag = s >> kFlagShift;
-          if (flag == 0) {
-            if (++spins > kSpinLimit) {
-              atomicOr(err, kStatusSpinLimit);
-              break;
-            }
-            __nanosleep(64);
-            continue;
+    uint32_t excl = 0;
+    if (tile == 0) {
+      if (lane == 0) st_relaxed_u64(&status[0], kFlagIncl | (uint64_t)blockTotal);
+    } else {
+      if (lane == 0) st_relaxed_u64(&status[tile], kFlagAgg | (uint64_t)blockTotal);
+      // warp-wide look-back: lane j reads predecessor pred - j, so one
+      // round trip covers 32 predecessors; the nearest inclusive prefix
+      // ends the walk, aggregates before it are summed
+      int64_t pred = (int64_t)tile - 1;
+      uint32_t spins = 0;
+      for (;;) {
+        const int64_t p = pred - lane;
+        const uint64_t st = p >= 0 ? ld_relaxed_u64(&status[p]) : kFlagIncl;
+        const uint32_t flag = (uint32_t)(st >> kFlagShift);
+        const uint32_t inclMask = __ballot_sync(0xffffffffu, flag == 2u);
+        const uint32_t zeroMask = __ballot_sync(0xffffffffu, flag == 0u);
+        const int firstIncl = inclMask ? __ffs(inclMask) - 1 : 32;
+        const int firstZero = zeroMask ? __ffs(zeroMask) - 1 : 32;
+        // lanes up to and including the prefix, or up to the first gap
+        const int take = firstIncl < firstZero ? firstIncl + 1 : firstZero;
+        excl += __reduce_add_sync(0xffffffffu, lane < take ? (uint32_t)(st & kValueMask) : 0u);
+        if (firstIncl < firstZero) break; // reached an inclusive prefix
+        pred -= take;
+        if (take == 0) {
+          if (++spins > kSpinLimit) {
+            if (lane == 0) atomicOr(err, kStatusSpinLimit);
+            break;
           }
-          excl += s & kValueMask;
-          if (flag == 2) break;
-          --pred;
+          __nanosleep(64);
         }
-        st_relaxed_u64(&status[tile], kFlagIncl | ((excl + blockTotal) & kValueMask));
       }
+      if (lane == 0)
+        st_relaxed_u64(&status[tile], kFlagIncl | ((uint64_t)(excl + blockTotal) & kValueMask));
+    }
+    if (lane == 0) {
       s_excl = excl;
       if (total && tile == numTiles - 1) *total = (uint32_t)(excl + blockTotal);
     }
@@ -250,22 +260,38 @@ __global__ void __launch_bounds__(kSortThreads)
       st_relaxed_u32(my, (2u << kRFlagShift) | count);
     } else {
       st_relaxed_u32(my, (1u << kRFlagShift) | count);
+      // look back over kLookBack predecessors per round trip (independent
+      // loads in flight); tile 0 is always inclusive, so the walk ends
+      // before it would read below tile 0
+      constexpr int kLookBack = 8;
       int pred = (int)tile - 1;
       uint32_t spins = 0;
-      while (pred >= 0) {
-        const uint32_t s = ld_relaxed_u32(status + (size_t)pred * 256 + d);
-        const uint32_t flag = s >> kRFlagShift;
-        if (flag == 0) {
+      for (;;) {
+        uint32_t w[kLookBack];
+#pragma unroll
+        for (int j = 0; j < kLookBack; ++j)
+          w[j] = pred - j >= 0 ? ld_relaxed_u32(status + (size_t)(pred - j) * 256 + d)
+                               : (2u << kRFlagShift);
+        int take = 0;
+        bool done = false;
+#pragma unroll
+        for (int j = 0; j < kLookBack; ++j) {
+          if (done || take < j) continue; // stopped at a gap or the prefix
+          const uint32_t flag = w[j] >> kRFlagShift;
+          if (flag == 0) continue;
+          excl += w[j] & kRValueMask;
+          ++take;
+          done = flag == 2;
+        }
+        if (done) break;
+        pred -= take;
+        if (take == 0) {
           if (++spins > kSpinLimit) {
             atomicOr(err, kStatusSpinLimit);
             break;
           }
           __nanosleep(32);
-          continue;
         }
-        excl += s & kRValueMask;
-        if (flag == 2) break;
-        --pred;
       }
       st_relaxed_u32(my, (2u << kRFlagShift) | ((excl + count) & kRValueMask));
     }
