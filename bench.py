@@ -54,6 +54,9 @@ WORKLOAD = {
 }
 # Algorithmic FLOPs per interaction (GPU Gems 3 ch. 31 convention).
 FLOP_PER_INTERACTION = 20.0
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_forces
+# launch on the two-disc 1M workload, from an ncu capture of its third launch.
+FORCE_TRAFFIC_BYTES = 23.70304e6
 
 
 def parse():
@@ -423,7 +426,9 @@ def run_b200(args):
             "kernel": "k_forces (warp-cooperative traversal)",
             "bound": "fp32", "achieved": achieved, "peak": peak,
             "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
-            "traffic": None,
+            "traffic": FORCE_TRAFFIC_BYTES if n == N_BODIES else None,
+            "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one "
+                            "launch, ncu capture at step 3 (a constant)",
             "peak_note": "FP32 FMA peak measured live by a probe kernel "
                          "(MEASURED_PEAKS.json holds no FP32 figure)",
             "flops_per_launch": flops, "launch_ms": force_ms,
