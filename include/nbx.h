@@ -242,7 +242,7 @@ int nbx_step_kernel_count(nbx_handle *h, uint32_t *kernels);
 
 /* Interactions of the traversal over the last tree for every body:
  * out5 = {accepted nodes with mass > 0, leaf body terms, visited nodes,
- * warp iterations, node-tile loads}. */
+ * warp iterations, leaf chunks staged (up to 32 bodies each)}. */
 int nbx_interaction_count(nbx_handle *h, double *out5);
 
 /* FP32 FMA throughput of the current device (TFLOP/s, 2 flops per FMA),

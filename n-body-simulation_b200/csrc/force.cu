@@ -11,10 +11,10 @@
 // The warp cooperates through the depth-first preorder layout (build.cu):
 // along every lane's walk the preorder position only increases (descend =
 // +1, skip = +subtree size), so the warp always serves the smallest
-// position any lane is waiting at.  The lanes at that node evaluate it
-// together from one shared-memory copy; tiles of the next 32 nodes are
-// staged into shared memory with one coalesced load, and a leaf's bodies
-// likewise, so the walk does not pay a dependent global load per node.
+// position any lane is waiting at.  The node's record is read once per
+// warp (one broadcast load through L1; staging 32-node tiles in shared
+// memory measured 9-11% slower for the extra per-iteration bookkeeping);
+// a leaf's bodies are staged in shared memory with one coalesced load.
 //
 // kExact = true evaluates every float operation as the reference writes
 // it (no FMA contraction, IEEE reciprocal): the result is bit-identical to
@@ -121,8 +121,6 @@ __global__ void __launch_bounds__(kForceBlock)
              const MlpDev *__restrict__ mlp = nullptr, float bandSq = 0.0f,
              float eps = 0.0f, const float2 *__restrict__ query = nullptr,
              uint32_t nQuery = 0, float2 *__restrict__ queryAcc = nullptr) {
-  __shared__ float4 sA[kWarps][32];
-  __shared__ int4 sB[kWarps][32];
   __shared__ float4 sBody[kWarps][32];
   __shared__ MlpDev sW;
   __shared__ __nv_bfloat16 sStage[kCorr == 1 ? kWarps : 1][32][16];
@@ -133,7 +131,6 @@ __global__ void __launch_bounds__(kForceBlock)
   }
   const int lane = threadIdx.x & 31;
   const int w = threadIdx.x >> 5;
-  const uint32_t totalNodes = S.counters[4];
   const uint32_t warpsTotal = (gridDim.x * blockDim.x) >> 5;
   // query points (instance 0's tree) instead of the bodies, if given
   const uint32_t nTargets = query ? nQuery : S.n;
@@ -157,25 +154,14 @@ __global__ void __launch_bounds__(kForceBlock)
       if (G.travCount > 0) cur = G.nodeBase;
     }
     float ax = 0.0f, ay = 0.0f;
-    uint32_t nFar = 0, nNear = 0, nVisit = 0, nIter = 0, nTile = 0;
-    // k - tileBase >= 32 (unsigned) forces the first tile load
-    uint32_t tileBase = 0xffffffe0u;
+    uint32_t nFar = 0, nNear = 0, nVisit = 0, nIter = 0, nChunk = 0;
     for (;;) {
       const uint32_t k = __reduce_min_sync(0xffffffffu, cur);
       if (k == kDone) break;
       if (kCount) ++nIter;
-      if (k - tileBase >= 32u) {
-        if (kCount) ++nTile;
-        tileBase = k;
-        const uint32_t g = k + lane;
-        if (g < totalNodes) {
-          sA[w][lane] = S.tA[g];
-          sB[w][lane] = S.tB[g];
-        }
-        __syncwarp();
-      }
-      const float4 A = sA[w][k - tileBase];
-      const int4 B = sB[w][k - tileBase];
+      // k is the same for the whole warp: one broadcast load through L1
+      const float4 A = __ldg(&S.tA[k]);
+      const int4 B = __ldg(&S.tB[k]);
       // the node after k's subtree (kDone past the instance's last node)
       const uint32_t nxt = (uint32_t)B.x;
       // every lane evaluates the node; only the lanes waiting at it use it
@@ -242,6 +228,7 @@ __global__ void __launch_bounds__(kForceBlock)
         const uint32_t bEnd = b1 <= S.n ? b1 : S.n; // defensive bound
         for (uint32_t base = b0; base < bEnd; base += 32) {
           const uint32_t cnt = min(32u, bEnd - base);
+          if (kCount) ++nChunk;
           __syncwarp();
           if ((uint32_t)lane < cnt) sBody[w][lane] = S.xym[base + lane];
           __syncwarp();
@@ -271,7 +258,7 @@ __global__ void __launch_bounds__(kForceBlock)
         atomicAdd(&counts[1], nn);
         atomicAdd(&counts[2], v);
         atomicAdd(&counts[3], (unsigned long long)nIter);
-        atomicAdd(&counts[4], (unsigned long long)nTile);
+        atomicAdd(&counts[4], (unsigned long long)nChunk);
       }
     } else if (valid) {
       if (query) queryAcc[i] = make_float2(ax, ay);

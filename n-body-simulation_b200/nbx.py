@@ -337,7 +337,7 @@ class Handle:
         out = np.zeros(5, np.float64)
         self._c(lib().nbx_interaction_count(self.h, out))
         return {"far": out[0], "near": out[1], "visits": out[2],
-                "warp_iters": out[3], "tile_loads": out[4]}
+                "warp_iters": out[3], "leaf_chunks": out[4]}
 
     def profile_step(self) -> dict:
         """One eager step; milliseconds per stage."""
