@@ -54,6 +54,11 @@ WORKLOAD = {
 }
 # Algorithmic FLOPs per interaction (GPU Gems 3 ch. 31 convention).
 FLOP_PER_INTERACTION = 20.0
+# Compulsory HBM bytes per body-step of every phase except the force pass
+# (FP32 state; one read + one write where a phase must move the data):
+# integrate 40, bounds 8, Morton 20, one sort pass 24, gather 56,
+# build + upward ~33, collision 88.
+ALG_BYTES_PER_BODY_STEP = 285.0 - 16.0  # the force pass's 16 B excluded
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_forces
 # launch on the two-disc 1M workload, from an ncu capture of its third launch.
 FORCE_TRAFFIC_BYTES = 23.70304e6
@@ -243,6 +248,54 @@ def forms_leg(nbx, torch, sim, n, local, ids, args):
     return out
 
 
+NAIVE_N = 1 << 18
+
+
+def naive_leg(nbx, torch, local, args):
+    """The direct all-pairs law (force_law = 1, NaiveSimulation) on a
+    2^18-body disc: a second roofline anchor (pure FP32/MUFU issue, n(n-1)
+    interactions per step, 20 FLOP each), against the reference's own
+    OpenMP NaiveSimulation on a smaller disc."""
+    n = NAIVE_N
+    sim = nbx.Simulation(nbx.uniform_disc(n), force_law=1, device=local)
+    stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+    sim.step(3)
+    sim.sync()
+    steps = 10
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step_timed(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    fms = sim.force_times(steps)
+    inter = float(n) * (n - 1)
+    tflops = FLOP_PER_INTERACTION * inter / (float(fms.mean()) * 1e-3) / 1e12
+    peak = nbx.fp32_peak_tflops()
+    rng = np.random.default_rng(12345)
+    err, _ = sim.force_error(rng.choice(n, 1024, replace=False).astype(np.uint32))
+    sim.close()
+    res = {"bodies": n, "steps": steps, "ms_per_step": ms,
+           "body_steps_per_s": n / (ms * 1e-3),
+           "force_ms": float(fms.mean()), "interactions_per_s": inter / (float(fms.mean()) * 1e-3),
+           "achieved_tflops": tflops, "peak_tflops": peak,
+           "frac": tflops / peak if peak else None,
+           "force_error_fp64_p99": err["p99"]}
+    try:  # the reference's own NaiveSimulation (OpenMP, its flags), smaller disc
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from oracle import Reference
+        R = Reference("omp")
+        nc = 1 << 15
+        _, cms = R.naive_simulate(nbx.uniform_disc(nc), steps=2)
+        res["reference_cpu"] = {"bodies": nc, "ms_per_step": cms / 2,
+                                "interactions_per_s": nc * (nc - 1) / (cms / 2 * 1e-3),
+                                "cores": R.threads()}
+    except Exception as ex:  # reference build absent
+        res["reference_cpu"] = {"unavailable": str(ex)}
+    return res
+
+
 def ensemble_leg(nbx, torch, world, rank, local, dist, args):
     """512 discs of log-uniform size in [2000, 200000] advanced by one
     handle, against looping the single-instance solver over the same
@@ -363,6 +416,15 @@ def run_b200(args):
     achieved = (FLOP_PER_INTERACTION * inter_steps.sum()
                 / (force_ms_steps.astype(np.float64).sum() * 1e-3) / 1e12)
     peak = nbx.fp32_peak_tflops()
+    # the rest of the step against the measured HBM copy bandwidth
+    hbm_peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            hbm_peak = float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        pass
+    other_ms = ms - force_ms
+    other_gbs = ALG_BYTES_PER_BODY_STEP * n / (other_ms * 1e-3) / 1e9
 
     # force error against the FP64 direct sum on 4096 sampled bodies
     rng = np.random.default_rng(12345)
@@ -399,6 +461,7 @@ def run_b200(args):
     learned = forms_leg(nbx, torch, sim, n, local, ids, args) if not args.quick else None
     sim_keep = sim
     ens = ensemble_leg(nbx, torch, world, rank, local, dist, args) if not args.quick else None
+    naive = naive_leg(nbx, torch, local, args) if not args.quick else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -441,6 +504,15 @@ def run_b200(args):
                       "interactions per step",
             "replay_bit_identical": replay_same,
         },
+        "roofline_other_phases": {
+            "bound": "hbm", "achieved": other_gbs, "peak": hbm_peak,
+            "unit": "GB/s", "frac": other_gbs / hbm_peak if hbm_peak else None,
+            "algorithmic_bytes_per_body_step": ALG_BYTES_PER_BODY_STEP,
+            "ms_per_step": other_ms,
+            "note": "step time minus the event-timed force pass; compulsory "
+                    "bytes of integrate, collision, bounds, Morton, one sort "
+                    "pass, gather, build; peak of measured (MEASURED_PEAKS.json "
+                    "hbm_gbs)"},
         "force_error_fp64": {"p50": err_stats["median"], "p99": err_stats["p99"],
                              "max": err_stats["max"], "samples": 4096},
         "interactions_per_s": (inter["far"] + inter["near"]) * 1e3 / ms,
@@ -451,6 +523,8 @@ def run_b200(args):
         line["learned_theta"] = learned
     if ens is not None:
         line["ensemble"] = ens
+    if naive is not None:
+        line["naive"] = naive
     if cpu is not None:
         line["cpu_baseline"] = cpu
     if rank == 0:

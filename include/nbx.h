@@ -71,6 +71,12 @@ typedef struct nbx_params {
   int32_t device;         /* CUDA device ordinal; -1 = the current device */
   float mlp_band;         /* learned correction on accepted cells with
                              size/distance >= mlp_band (default 0.5) */
+  int32_t force_law;      /* 0: Barnes-Hut tree (Simulation, default);
+                             1: direct all-pairs sum with the Plummer law of
+                             NaiveSimulation::attract
+                             (src/naive/NaiveSimulation.cpp:17-57,
+                             src/cuda/CudaNaive.cu:17-57); no tree is built,
+                             use_mlp must be 0 */
 } nbx_params;
 
 typedef struct nbx_handle nbx_handle;
@@ -191,9 +197,11 @@ int nbx_nbs2_close(nbx_nbs2 *f);
 
 /* --- FP64 checks --- */
 
-/* FP64 direct-sum accelerations with the tree's force law (no softening
- * change, eps = params.epsilon) for bodies at the given current indices
- * (exactTreeLawForces, CheckCuda.cu:453-475). */
+/* FP64 direct-sum accelerations for bodies at the given current indices,
+ * over the other bodies of each target's own instance, with the handle's
+ * force law: the tree's m d / (|d| (d^2 + eps^2)) (exactTreeLawForces,
+ * CheckCuda.cu:453-475), or with force_law = 1 the Plummer law
+ * m d / (d^2 + eps^2)^1.5; eps = params.epsilon. */
 int nbx_direct_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m,
                     double *ax, double *ay);
 

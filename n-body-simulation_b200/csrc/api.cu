@@ -23,6 +23,8 @@ void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
                   SortScratch &sort);
 void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
                    const MlpDev *mlp, float band, int corr);
+DevState launch_naive_gather(cudaStream_t s, const DevState &S);
+void launch_naive_forces(cudaStream_t s, const DevState &S, bool exact);
 void mlp_harvest(cudaStream_t s, const DevState &S, const uint32_t *targets,
                  uint32_t nt, float theta, float band, float eps, uint2 *items,
                  uint32_t cap, uint32_t *count, float *rows);
@@ -41,8 +43,9 @@ double fp32_fma_peak_tflops(cudaStream_t s);
 void launch_query_forces(cudaStream_t s, const DevState &S, bool exact,
                          const float2 *query, uint32_t nq, float2 *out);
 void launch_direct_fp64(cudaStream_t s, const float4 *pv, const float2 *mr,
-                        uint32_t n, const uint32_t *targets, uint32_t m,
-                        double eps, double2 *partial, double *ax, double *ay);
+                        uint32_t n, const uint32_t *targets, const uint2 *ranges,
+                        uint32_t m, double eps, int plummer, double2 *partial,
+                        double *ax, double *ay);
 size_t direct_partial_elems(uint32_t m);
 void launch_energy_momentum(cudaStream_t s, const float4 *pv, const float2 *mr,
                             uint32_t n, double *part, double *out);
@@ -144,7 +147,8 @@ struct nbx_handle {
   bool timedValid = false;
   bool timedCapture = false;
   bool uploaded = false;
-  bool treeValid = false;
+  bool treeValid = false;   // a Barnes-Hut tree of the current state exists
+  bool forceInput = false;  // S.xym holds the current state's bodies
   bool collideValid = false;
   bool idsChecked = false;     // ids verified to be per-instance permutations
   bool idsPermutation = false;
@@ -362,6 +366,15 @@ DevState enqueue_step(nbx_handle *h, cudaStream_t s, DevState S) {
   launch_integrate(s, S, true, S.collisions != 0);
   mark(s, "integrate");
   if (S.collisions) launch_collide(s, S, h->scan, h->sort);
+  if (h->params.force_law == 1) {
+    S = launch_naive_gather(s, S);
+    mark(s, "naive.gather");
+    if (h->timedCapture) cudaEventRecordWithFlags(h->forceMark[0], s, cudaEventRecordExternal);
+    launch_naive_forces(s, S, h->params.exact_math != 0);
+    if (h->timedCapture) cudaEventRecordWithFlags(h->forceMark[1], s, cudaEventRecordExternal);
+    mark(s, "forces");
+    return S;
+  }
   launch_build(s, S, h->scan, h->sort);
   if (h->timedCapture) cudaEventRecordWithFlags(h->forceMark[0], s, cudaEventRecordExternal);
   launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
@@ -385,6 +398,13 @@ void destroy_graphs(nbx_handle *h) {
     h->graphTSrc[p] = nullptr;
   }
   h->timedValid = false;
+}
+
+// Flags after a whole step: the naive law builds no tree.
+void after_step(nbx_handle *h) {
+  h->treeValid = h->params.force_law == 0;
+  h->forceInput = true;
+  h->collideValid = h->params.collisions != 0;
 }
 
 // Step graphs with the force launch bracketed by event-record nodes (kept
@@ -484,7 +504,8 @@ int check_status(nbx_handle *h) {
 bool valid_params(const nbx_params *p) {
   return p && p->dt == p->dt && p->theta >= 0.0f && p->epsilon >= 0.0f &&
          p->leaf_capacity >= 1 && p->leaf_capacity <= 64 && p->use_mlp >= 0 &&
-         p->use_mlp <= 2;
+         p->use_mlp <= 2 && (p->force_law == 0 || p->force_law == 1) &&
+         !(p->force_law == 1 && p->use_mlp != 0);
 }
 
 } // namespace
@@ -508,6 +529,7 @@ int nbx_params_default(nbx_params *p) {
   p->force_blocks = 0;
   p->device = -1;
   p->mlp_band = 0.5f;
+  p->force_law = 0;
   return NBX_OK;
 }
 
@@ -638,6 +660,7 @@ int nbx_upload_bodies(nbx_handle *h, const nbx_body *bodies, size_t n) {
   h->idsChecked = false;
   h->uploaded = true;
   h->treeValid = false;
+  h->forceInput = false;
   h->collideValid = false;
   return NBX_OK;
 }
@@ -694,8 +717,7 @@ int nbx_step(nbx_handle *h, uint32_t steps) {
     NBX_CUDA(h, cudaGraphLaunch(h->graph[h->cur], h->stream));
     h->cur ^= 1;
   }
-  h->treeValid = true;
-  h->collideValid = h->params.collisions != 0;
+  after_step(h);
   return NBX_OK;
 }
 
@@ -727,8 +749,7 @@ int nbx_step_timed(nbx_handle *h, uint32_t steps) {
     h->cur ^= 1;
   }
   h->timedSteps = steps;
-  h->treeValid = true;
-  h->collideValid = h->params.collisions != 0;
+  after_step(h);
   return NBX_OK;
 }
 
@@ -769,20 +790,42 @@ int nbx_phase(nbx_handle *h, int phase) {
     h->collideValid = true;
     break;
   case NBX_PHASE_BUILD:
+    if (h->params.force_law == 1) { // no tree: the identity gather
+      S = launch_naive_gather(s, S);
+      h->cur ^= 1;
+      h->treeValid = false;
+      h->forceInput = true;
+      break;
+    }
     launch_build(s, S, h->scan, h->sort);
     h->cur ^= 1;
     h->treeValid = true;
+    h->forceInput = true;
     break;
   case NBX_PHASE_FORCES:
+    if (h->params.force_law == 1) {
+      if (!h->forceInput) return fail(h, NBX_ERR_STATE, "no force input gathered");
+      launch_naive_forces(s, S, h->params.exact_math != 0);
+      break;
+    }
     if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
     launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
                   h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
                   h->params.use_mlp);
     break;
   case NBX_PHASE_ATTRACT:
+    if (h->params.force_law == 1) {
+      S = launch_naive_gather(s, S);
+      h->cur ^= 1;
+      h->treeValid = false;
+      h->forceInput = true;
+      launch_naive_forces(s, S, h->params.exact_math != 0);
+      break;
+    }
     launch_build(s, S, h->scan, h->sort);
     h->cur ^= 1;
     h->treeValid = true;
+    h->forceInput = true;
     launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
                   h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
                   h->params.use_mlp);
@@ -790,8 +833,7 @@ int nbx_phase(nbx_handle *h, int phase) {
   case NBX_PHASE_STEP:
     enqueue_step(h, s, S);
     h->cur ^= 1;
-    h->treeValid = true;
-    h->collideValid = S.collisions != 0;
+    after_step(h);
     break;
   default:
     return fail(h, NBX_ERR_ARG, "unknown phase");
@@ -908,14 +950,27 @@ int nbx_direct_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m, double *
     h->dTargets = nullptr;
     h->dPartialTargets = 0;
     NBX_CUDA(h, cudaMalloc(&h->dPartial, direct_partial_elems(m) * sizeof(double2) + 16 * m));
-    NBX_CUDA(h, cudaMalloc(&h->dTargets, 4ull * m));
+    // targets (u32), then 8-byte aligned source ranges (uint2)
+    NBX_CUDA(h, cudaMalloc(&h->dTargets, 4ull * (m + 1) + 8ull * m));
     h->dPartialTargets = m;
   }
   double *dOut = reinterpret_cast<double *>(h->dPartial + direct_partial_elems(h->dPartialTargets));
-  NBX_CUDA(h, cudaMemcpyAsync(h->dTargets, targets, 4ull * m, cudaMemcpyHostToDevice, h->stream));
+  // each target's sources: the bodies of its own instance
+  uint2 *dRanges = reinterpret_cast<uint2 *>(h->dTargets + ((h->dPartialTargets + 1) & ~1u));
+  std::vector<uint32_t> staged(3ull * m);
+  for (uint32_t k = 0; k < m; ++k) {
+    const auto it = std::upper_bound(h->segStart.begin(), h->segStart.end(), targets[k]);
+    const size_t sg = (size_t)(it - h->segStart.begin()) - 1;
+    staged[k] = targets[k];
+    staged[m + 2 * k] = h->segStart[sg];
+    staged[m + 2 * k + 1] = h->segStart[sg] + h->segCount[sg];
+  }
+  NBX_CUDA(h, cudaMemcpyAsync(h->dTargets, staged.data(), 4ull * m, cudaMemcpyHostToDevice, h->stream));
+  NBX_CUDA(h, cudaMemcpyAsync(dRanges, staged.data() + m, 8ull * m, cudaMemcpyHostToDevice, h->stream));
   const DevState S = h->state();
-  launch_direct_fp64(h->stream, S.pv, S.mr, h->n, h->dTargets, m, h->params.epsilon,
-                     h->dPartial, dOut, dOut + m);
+  launch_direct_fp64(h->stream, S.pv, S.mr, h->n, h->dTargets, dRanges, m,
+                     h->params.epsilon, h->params.force_law == 1 ? 1 : 0, h->dPartial,
+                     dOut, dOut + m);
   NBX_CUDA(h, cudaGetLastError());
   NBX_CUDA(h, cudaMemcpyAsync(ax, dOut, 8ull * m, cudaMemcpyDeviceToHost, h->stream));
   NBX_CUDA(h, cudaMemcpyAsync(ay, dOut + m, 8ull * m, cudaMemcpyDeviceToHost, h->stream));
@@ -985,8 +1040,7 @@ int nbx_profile_step(nbx_handle *h, uint32_t max_marks, char *labels,
   enqueue_step(h, s, h->state());
   g_marks = nullptr;
   h->cur ^= 1;
-  h->treeValid = true;
-  h->collideValid = h->params.collisions != 0;
+  after_step(h);
   cudaError_t e = cudaStreamSynchronize(s);
   const uint32_t segs = marks.count > 0 ? (uint32_t)marks.count - 1 : 0;
   *count = segs;
@@ -1297,6 +1351,7 @@ int nbx_autotune(nbx_handle *h, int allowLeaf, uint32_t steps, nbx_params *best,
   scratch_free(h, sv);
   if (e != cudaSuccess && !rc) rc = cuda_fail(h, e, "autotune");
   h->treeValid = false;
+  h->forceInput = false;
   h->collideValid = false;
   *best = h->params;
   if (bestMs) *bestMs = bestT;

@@ -15,11 +15,14 @@ constexpr int kDirectChunks = 64;
 __global__ void __launch_bounds__(kDirectThreads)
     k_direct_partial(const float4 *__restrict__ pv, const float2 *__restrict__ mr,
                      uint32_t n, const uint32_t *__restrict__ targets,
-                     uint32_t m, double eSq, double2 *__restrict__ partial) {
+                     const uint2 *__restrict__ ranges, uint32_t m, double eSq,
+                     int plummer, double2 *__restrict__ partial) {
   __shared__ float4 sSrc[kDirectThreads];
   const uint32_t t = blockIdx.x * kDirectThreads + threadIdx.x;
   const bool valid = t < m;
   const uint32_t ti = valid ? targets[t] : 0u;
+  // sources: the target's own instance
+  const uint2 rg = valid ? ranges[t] : make_uint2(0u, 0u);
   double x = 0.0, y = 0.0;
   if (valid) {
     const float4 p = pv[ti];
@@ -42,12 +45,16 @@ __global__ void __launch_bounds__(kDirectThreads)
     if (valid) {
       for (uint32_t k = 0; k < cnt; ++k) {
         const float4 s = sSrc[k];
-        if (__float_as_uint(s.w) == ti) continue;
+        const uint32_t sj = __float_as_uint(s.w);
+        if (sj == ti || sj < rg.x || sj >= rg.y) continue;
         const double dx = (double)s.x - x;
         const double dy = (double)s.y - y;
         const double dSq = dx * dx + dy * dy;
         if (dSq == 0.0) continue;
-        const double f = (double)s.z / (sqrt(dSq) * (dSq + eSq));
+        // tree law m d / (|d| (d^2 + eps^2)); Plummer m d / (d^2 + eps^2)^1.5
+        const double q = dSq + eSq;
+        const double f = plummer ? (double)s.z / (q * sqrt(q))
+                                 : (double)s.z / (sqrt(dSq) * q);
         ax += dx * f;
         ay += dy * f;
       }
@@ -132,12 +139,13 @@ __global__ void k_energy_final(const double *__restrict__ part, int blocks,
 
 // partial must hold kDirectChunks * m double2.
 void launch_direct_fp64(cudaStream_t s, const float4 *pv, const float2 *mr,
-                        uint32_t n, const uint32_t *targets, uint32_t m,
-                        double eps, double2 *partial, double *ax, double *ay) {
+                        uint32_t n, const uint32_t *targets, const uint2 *ranges,
+                        uint32_t m, double eps, int plummer, double2 *partial,
+                        double *ax, double *ay) {
   if (m == 0) return;
   dim3 grid((m + kDirectThreads - 1) / kDirectThreads, kDirectChunks);
-  k_direct_partial<<<grid, kDirectThreads, 0, s>>>(pv, mr, n, targets, m,
-                                                   eps * eps, partial);
+  k_direct_partial<<<grid, kDirectThreads, 0, s>>>(pv, mr, n, targets, ranges, m,
+                                                   eps * eps, plummer, partial);
   k_direct_reduce<<<(m + 255) / 256, 256, 0, s>>>(partial, m, kDirectChunks, ax,
                                                   ay);
 }

@@ -10,7 +10,8 @@
 // cluster/times.sh read its output unchanged.  The state stays on the GPU;
 // frames are copied back in id order only when written (as sim_cuda).
 // Optional trailing flags: --theta= --eps= --dt= --leaf= --collisions=0/1
-// --scenario=disc|two|cold --seed= --exact=0/1.
+// --scenario=disc|two|cold --seed= --exact=0/1 --naive=0/1 (the direct
+// all-pairs law of sim_naive / sim_cuda_naive, MainNaive.cpp).
 #include "nbx.h"
 
 #include <chrono>
@@ -51,6 +52,7 @@ int main(int argc, char **argv) {
     else if (flag(a, "leaf", v)) p.leaf_capacity = std::stoi(v);
     else if (flag(a, "collisions", v)) p.collisions = std::stoi(v);
     else if (flag(a, "exact", v)) p.exact_math = std::stoi(v);
+    else if (flag(a, "naive", v)) p.force_law = std::stoi(v) ? 1 : 0;
     else if (flag(a, "scenario", v)) scenario = v;
     else if (flag(a, "seed", v)) seed = (uint32_t)std::stoul(v);
     else {

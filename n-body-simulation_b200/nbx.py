@@ -54,7 +54,7 @@ class Params(C.Structure):
                 ("exact_math", C.c_int32), ("use_mlp", C.c_int32),
                 ("node_factor", C.c_float), ("pair_factor", C.c_float),
                 ("force_blocks", C.c_int32), ("device", C.c_int32),
-                ("mlp_band", C.c_float)]
+                ("mlp_band", C.c_float), ("force_law", C.c_int32)]
 
 
 class NbxError(RuntimeError):

@@ -874,3 +874,45 @@ double orc_potential_fp64(size_t n, const orc_body *b, double epsilon) {
   }
   return s + c;
 }
+
+void orc_naive_forces(size_t n, const float *x, const float *y, const float *m,
+                      float epsilon, float *ax, float *ay) {
+  const float eSq = epsilon * epsilon;
+  for (size_t i = 0; i < n; ++i) {
+    float sx = 0.0f, sy = 0.0f;
+    const float xi = x[i], yi = y[i];
+    for (size_t j = 0; j < n; ++j) {
+      if (i == j) continue;
+      const float dx = x[j] - xi, dy = y[j] - yi;
+      const float dSq = dx * dx + dy * dy;
+      const float invSoft = 1.0f / (dSq + eSq);
+      const float invDist = 1.0f / sqrtf(dSq + eSq);
+      const float factor = m[j] * invDist * invSoft;
+      sx += dx * factor;
+      sy += dy * factor;
+    }
+    ax[i] = sx;
+    ay[i] = sy;
+  }
+}
+
+int orc_naive_step(size_t n, orc_body *b, float dt, float epsilon, int collisions) {
+  orc_integrate(n, b, dt);
+  if (collisions && orc_collide(n, b) < 0) return -1;
+  if (n == 0) return 0;
+  float *x = (float *)malloc(5 * n * sizeof(float));
+  if (!x) return -1;
+  float *y = x + n, *m = x + 2 * n, *ax = x + 3 * n, *ay = x + 4 * n;
+  for (size_t i = 0; i < n; ++i) {
+    x[i] = b[i].px;
+    y[i] = b[i].py;
+    m[i] = b[i].mass;
+  }
+  orc_naive_forces(n, x, y, m, epsilon, ax, ay);
+  for (size_t i = 0; i < n; ++i) {
+    b[i].ax = ax[i];
+    b[i].ay = ay[i];
+  }
+  free(x);
+  return 0;
+}

@@ -101,6 +101,17 @@ int64_t orc_collide(size_t n, orc_body *b);
 int orc_step(size_t n, orc_body *b, float dt, float theta, float epsilon,
              int leafCapacity, int collisions);
 
+/* Direct all-pairs accelerations, NaiveSimulation::attract
+ * (src/naive/NaiveSimulation.cpp:17-57): for each i, over j != i in index
+ * order, d = pos_j - pos_i, s = |d|^2 + eps^2,
+ * acc += d * (m_j * (1/sqrt(s)) * (1/s)), IEEE single precision. */
+void orc_naive_forces(size_t n, const float *x, const float *y, const float *m,
+                      float epsilon, float *ax, float *ay);
+
+/* One NaiveSimulation::step (NaiveSimulation.cpp:10-15): iterate -> collide
+ * -> naive attract; bodies keep their order.  Returns 0, or -1. */
+int orc_naive_step(size_t n, orc_body *b, float dt, float epsilon, int collisions);
+
 /* FP64 direct sum with the tree's force law for the given targets
  * (exactTreeLawForces, src/cuda/CheckCuda.cu:453-475; eps generalised). */
 void orc_direct_fp64(size_t n, const float *x, const float *y, const float *m,

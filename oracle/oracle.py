@@ -106,6 +106,11 @@ class Oracle:
         L.orc_step.argtypes = [C.c_size_t, _bodyp, C.c_float, C.c_float,
                                C.c_float, C.c_int, C.c_int]
         L.orc_step.restype = C.c_int
+        L.orc_naive_forces.argtypes = [C.c_size_t, _f32p, _f32p, _f32p,
+                                       C.c_float, _f32p, _f32p]
+        L.orc_naive_step.argtypes = [C.c_size_t, _bodyp, C.c_float, C.c_float,
+                                     C.c_int]
+        L.orc_naive_step.restype = C.c_int
         L.orc_direct_fp64.argtypes = [C.c_size_t, _f32p, _f32p, _f32p,
                                       C.c_double, C.c_size_t, _u32p, _f64p,
                                       _f64p]
@@ -223,6 +228,22 @@ class Oracle:
                 raise RuntimeError("oracle step failed")
         return b
 
+    def naive_forces(self, x, y, m, eps):
+        """NaiveSimulation::attract (NaiveSimulation.cpp:17-57)."""
+        x, y, m = (np.ascontiguousarray(v, np.float32) for v in (x, y, m))
+        ax = np.zeros(len(x), np.float32)
+        ay = np.zeros(len(x), np.float32)
+        self.L.orc_naive_forces(len(x), x, y, m, eps, ax, ay)
+        return ax, ay
+
+    def naive_step(self, b: np.ndarray, dt=0.05, eps=1.0, collisions=True, steps=1):
+        """NaiveSimulation::step (NaiveSimulation.cpp:10-15)."""
+        b = np.ascontiguousarray(b.copy())
+        for _ in range(steps):
+            if self.L.orc_naive_step(len(b), b, dt, eps, int(collisions)) != 0:
+                raise RuntimeError("oracle naive step failed")
+        return b
+
     def direct_fp64(self, b: np.ndarray, eps, targets):
         targets = np.ascontiguousarray(targets, np.uint32)
         ax = np.zeros(len(targets), np.float64)
@@ -262,6 +283,9 @@ class Reference:
         L.ref_simulate.argtypes = [C.c_size_t, _bodyp, C.c_float, C.c_float,
                                    C.c_float, C.c_int, C.c_int, C.c_int]
         L.ref_simulate.restype = C.c_double
+        L.ref_naive_attract.argtypes = [C.c_size_t, _bodyp]
+        L.ref_naive_simulate.argtypes = [C.c_size_t, _bodyp, C.c_float, C.c_int]
+        L.ref_naive_simulate.restype = C.c_double
         L.ref_morton.argtypes = [C.c_size_t, _f32p, _f32p, _f32p, _u64p]
         L.ref_build_tree.argtypes = [C.c_size_t, _u64p, _f32p, _f32p, _f32p,
                                      _f32p, C.c_int] + [_f32p] * 6 + \
@@ -303,6 +327,16 @@ class Reference:
         b = np.ascontiguousarray(b.copy())
         ms = self.L.ref_simulate(len(b), b, dt, theta, eps, leaf, steps,
                                  int(collisions))
+        return b, ms
+
+    def naive_attract(self, b):
+        b = np.ascontiguousarray(b.copy())
+        self.L.ref_naive_attract(len(b), b)
+        return b
+
+    def naive_simulate(self, b, dt=0.05, steps=1):
+        b = np.ascontiguousarray(b.copy())
+        ms = self.L.ref_naive_simulate(len(b), b, dt, steps)
         return b, ms
 
     def morton(self, x, y, root):

@@ -2,11 +2,13 @@
 //
 // TEST INFRASTRUCTURE ONLY.  oracle/Makefile compiles this file together
 // with the reference's own src/Simulation.cpp, src/QuadTree.cpp,
-// src/Collision.cpp and src/Utils.cpp (read in place, never copied) into
+// src/Collision.cpp, src/Utils.cpp and src/naive/NaiveSimulation.cpp (read
+// in place, never copied) into
 // oracle/_ref/.  It is used to pin the CPU restatement (nbody_oracle.c),
 // to write golden fixtures, and as the timed CPU baseline.  Nothing here
 // re-implements the reference: every call lands in the reference's code.
 #include "Collision.h"
+#include "NaiveSimulation.h"
 #include "QuadTree.h"
 #include "Simulation.h"
 #include "Utils.h"
@@ -90,6 +92,28 @@ double ref_simulate(std::size_t n, Body *b, float dt, float theta, float eps,
       sim.frame += 1;
     }
   }
+  const auto t1 = std::chrono::steady_clock::now();
+  std::memcpy(b, sim.bodies.data(), n * sizeof(Body));
+  return std::chrono::duration<double, std::milli>(t1 - t0).count();
+}
+
+// NaiveSimulation::attract (NaiveSimulation.cpp:17-57) on the given
+// bodies: writes their accelerations.
+void ref_naive_attract(std::size_t n, Body *b) {
+  NaiveSimulation sim(1);
+  sim.bodies = toVec(b, n);
+  sim.attract();
+  std::memcpy(b, sim.bodies.data(), n * sizeof(Body));
+}
+
+// `steps` NaiveSimulation::step() calls (iterate -> collide -> attract);
+// returns the wall time in ms.
+double ref_naive_simulate(std::size_t n, Body *b, float dt, int steps) {
+  NaiveSimulation sim(1);
+  sim.bodies = toVec(b, n);
+  sim.dt = dt;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int k = 0; k < steps; ++k) sim.step();
   const auto t1 = std::chrono::steady_clock::now();
   std::memcpy(b, sim.bodies.data(), n * sizeof(Body));
   return std::chrono::duration<double, std::milli>(t1 - t0).count();

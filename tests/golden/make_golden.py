@@ -81,6 +81,10 @@ def main():
     for theta in (1.0, 0.5):
         out, _ = Rp.simulate(small, theta=theta, steps=10)
         g[f"sim10_t{theta}"] = out
+    # NaiveSimulation: attract on the disc, 5 steps from a 1024-body disc
+    g["naive_acc"] = np.stack([Rp.naive_attract(small)["ax"], Rp.naive_attract(small)["ay"]])
+    g["naive_in"] = Ro.uniform_disc(1024, 3)
+    g["naive5"], _ = Rp.naive_simulate(g["naive_in"], steps=5)
     np.savez_compressed(OUT, **g)
     print("wrote", OUT, os.path.getsize(OUT), "bytes")
 

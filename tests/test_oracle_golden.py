@@ -82,3 +82,11 @@ def test_oracle_step_tracks_reference_simulation(oracle, golden):
         err = np.hypot(g["px"] - r["px"], g["py"] - r["py"]) / np.hypot(r["px"], r["py"])
         assert np.isfinite(err).all()
         assert np.median(err) < 1e-4 and err.max() < 1e-3, (np.median(err), err.max())
+
+
+def test_naive_forces_and_steps_bit_exact(oracle, golden):
+    """NaiveSimulation::attract / ::step (the reference's own outputs)."""
+    b = golden["sim_in"]
+    ax, ay = oracle.naive_forces(b["px"], b["py"], b["mass"], 1.0)
+    assert same_bits(np.stack([ax, ay]), golden["naive_acc"])
+    assert same_bits(oracle.naive_step(golden["naive_in"], steps=5), golden["naive5"])

@@ -41,3 +41,16 @@ def test_collide_and_step(oracle, ref, n):
     assert same_bits(out, ref.collide(st))
     q = oracle.quadtree_forces(st, 0.7, 1.0)
     assert same_bits(q, ref.quadtree_forces(st, 0.7, 1.0))
+
+
+@pytest.mark.parametrize("n", [1, 2, 257, 3000])
+def test_naive_forces_and_steps(oracle, ref, n):
+    """NaiveSimulation::attract and ::step restated (nbody_oracle.c) against
+    the reference's own NaiveSimulation.cpp, bit for bit."""
+    b = ref.uniform_disc(n)
+    r = ref.naive_attract(b)
+    ax, ay = oracle.naive_forces(b["px"], b["py"], b["mass"], 1.0)
+    assert same_bits(ax, r["ax"]) and same_bits(ay, r["ay"])
+    o = oracle.naive_step(b, steps=3)
+    r3, _ = ref.naive_simulate(b, steps=3)
+    assert same_bits(o, r3)
