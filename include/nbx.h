@@ -129,6 +129,20 @@ int nbx_download_bodies(nbx_handle *h, nbx_body *bodies, size_t n,
  * per step and returns; errors raised on the device surface at nbx_sync. */
 int nbx_step(nbx_handle *h, uint32_t steps);
 
+/* The viewer's attractor (CudaSimulation.cuh:9-15, attractorKernel
+ * CudaSimulation.cu:14-31): while active, every step adds to each body's
+ * acceleration the pull of a point mass at (x, y),
+ * d * mass / (sqrt(|d|^2 + 1e-12) * (|d|^2 + softening^2)), d = (x, y) - pos,
+ * after the gravitational sum.  Defaults: inactive, mass 1e6, softening 50.
+ * Takes effect from the next step enqueued; no graph is re-captured. */
+int nbx_set_attractor(nbx_handle *h, int active, float x, float y, float mass,
+                      float softening);
+
+/* CudaSimulation::reset (CudaSimulation.cu:40-49): replaces every body of a
+ * single-instance handle, any count, reallocating the device state for it.
+ * Parameters, the attractor and loaded network parameters are kept. */
+int nbx_reset(nbx_handle *h, const nbx_body *bodies, size_t n);
+
 /* nbx_step with the duration of each step's force pass recorded by CUDA
  * events on the handle's stream, around the force launch inside the step's
  * graph (the same kernels as nbx_step, plus two event records per step).
@@ -326,8 +340,34 @@ int nbx_two_discs(uint32_t n, uint32_t seed, float approach_fraction,
                   nbx_body *out);
 
 /* n unit-mass, radius-1 bodies at rest uniform in [-h, h]^2 with
- * h = 3*sqrt(n), mt19937(seed) (viewer/Scenarios.cpp:50-57). */
+ * h = 3*sqrt(n), mt19937(seed): the viewer's ColdSquare
+ * (viewer/Scenarios.cpp:50-57), = nbx_make_scenario(NBX_SCENARIO_COLD_SQUARE). */
 int nbx_cold_square(uint32_t n, uint32_t seed, nbx_body *out);
+
+/* The viewer's scenarios and edits (viewer/Scenarios.h:1-23), for
+ * injecting states into a handle without a GUI: edit a host copy, then
+ * nbx_reset() the handle with it (viewer/main.cpp:122-129).  Results are
+ * bit-identical to the viewer's build (its -O2 for these, -Ofast for
+ * uniformDisc). */
+enum {
+  NBX_SCENARIO_DISC = 0,         /* uniformDisc(n, seed) */
+  NBX_SCENARIO_TWO_GALAXIES = 1, /* two discs on a glancing course */
+  NBX_SCENARIO_COLD_SQUARE = 2   /* unit masses at rest, half-width 3 sqrt(n) */
+};
+/* makeScenario (Scenarios.cpp:28-62): n bodies, ids 0..n-1.  n >= 1 for a
+ * disc and n >= 2 for two galaxies (smaller sizes make the reference return
+ * more bodies than asked: uniformDisc(0) still holds its central body). */
+int nbx_make_scenario(int kind, uint32_t n, uint32_t seed, nbx_body *out);
+/* renumber (Scenarios.cpp:22-26): ids 0..n-1 in array order. */
+void nbx_renumber(nbx_body *bodies, size_t n);
+/* addHeavyBody (Scenarios.cpp:64-70): writes body n (the array must hold
+ * n + 1) at rest at (x, y); returns the new count. */
+size_t nbx_add_heavy_body(nbx_body *bodies, size_t n, float x, float y, float mass);
+/* addCluster (Scenarios.cpp:72-86): writes bodies n .. n+count-1 (unit
+ * mass and radius, velocity (vx, vy)) in a small disc around (x, y),
+ * mt19937(seed); returns the new count. */
+size_t nbx_add_cluster(nbx_body *bodies, size_t n, float x, float y, float vx,
+                       float vy, size_t count, uint32_t seed);
 
 /* Instance sizes of the batched ensemble: instance i has
  * round(exp(U(ln lo, ln hi))) bodies, U drawn from mt19937(i). */

@@ -165,6 +165,9 @@ struct nbx_handle {
   bool mlpLoaded = false;
   int mlpStep = 0;
   std::vector<void *> scratch; // grow-on-demand buffers (MLP data)
+  // attractor (CudaSimulation.cuh:9-15 defaults): {x, y, mass, softening},
+  // {active, 0, 0, 0}; mirrored into S.attr
+  float attrHost[8] = {0.0f, 0.0f, 1e6f, 50.0f, 0.0f, 0.0f, 0.0f, 0.0f};
 
   DevState state() const {
     DevState S = base;
@@ -315,7 +318,9 @@ int allocate(nbx_handle *h) {
   A(h->mlpV, kMlpParams);
   A(h->mlpGrad, kMlpParams + 1);
   A(h->mlpW, 1);
+  A(S.attr, 2);
 #undef A
+  NBX_CUDA(h, cudaMemcpy(S.attr, h->attrHost, sizeof(h->attrHost), cudaMemcpyHostToDevice));
   // bounds accumulators start empty
   std::vector<uint32_t> b(4 * ns);
   for (uint32_t s = 0; s < ns; ++s) {
@@ -762,6 +767,65 @@ int nbx_force_times(nbx_handle *h, float *ms, uint32_t count) {
   for (uint32_t k = 0; k < count; ++k)
     NBX_CUDA(h, cudaEventElapsedTime(&ms[k], h->forceEv[2 * k], h->forceEv[2 * k + 1]));
   return check_status(h);
+}
+
+int nbx_set_attractor(nbx_handle *h, int active, float x, float y, float mass,
+                      float softening) {
+  if (!h) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  const float v[8] = {x, y, mass, softening, active ? 1.0f : 0.0f, 0.0f, 0.0f, 0.0f};
+  std::memcpy(h->attrHost, v, sizeof(v));
+  // stream-ordered: steps enqueued before see the old attractor, later
+  // ones the new; the captured graphs read it from device memory
+  NBX_CUDA(h, cudaMemcpyAsync(h->base.attr, h->attrHost, sizeof(v),
+                              cudaMemcpyHostToDevice, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  return NBX_OK;
+}
+
+int nbx_reset(nbx_handle *h, const nbx_body *bodies, size_t n) {
+  if (!h || (!bodies && n) || n >= (1ull << 30)) return NBX_ERR_ARG;
+  if (h->nseg != 1)
+    return fail(h, NBX_ERR_ARG, "nbx_reset replaces the bodies of a single-instance handle");
+  cudaSetDevice(h->device);
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  // keep the network parameters across the reallocation (optimizer
+  // moments start again)
+  std::vector<float> mlp;
+  if (h->mlpLoaded) {
+    mlp.resize(kMlpParams);
+    NBX_CUDA(h, cudaMemcpy(mlp.data(), h->mlpP, kMlpParams * sizeof(float),
+                           cudaMemcpyDeviceToHost));
+  }
+  destroy_graphs(h);
+  for (void *v : h->allocs) cudaFree(v);
+  h->allocs.clear();
+  for (void *v : h->scratch) cudaFree(v);
+  h->scratch.clear();
+  if (h->hPinned) cudaFreeHost(h->hPinned);
+  if (h->dPartial) cudaFree(h->dPartial);
+  if (h->dTargets) cudaFree(h->dTargets);
+  h->hPinned = nullptr;
+  h->dPartial = nullptr;
+  h->dTargets = nullptr;
+  h->dPartialTargets = 0;
+  h->base = DevState{};
+  h->scan = ScanScratch{};
+  h->sort = SortScratch{};
+  h->cur = 0;
+  h->n = (uint32_t)n;
+  h->segStart.assign(1, 0u);
+  h->segCount.assign(1, (uint32_t)n);
+  h->uploaded = h->treeValid = h->forceInput = h->collideValid = false;
+  h->idsChecked = h->idsPermutation = false;
+  h->mlpLoaded = false;
+  h->timedSteps = 0;
+  int rc = allocate(h);
+  if (rc != NBX_OK) return rc;
+  sync_params(h);
+  if (!mlp.empty() && (rc = nbx_mlp_set_params(h, mlp.data(), kMlpParams)) != NBX_OK)
+    return rc;
+  return nbx_upload_bodies(h, bodies, n);
 }
 
 int nbx_sync(nbx_handle *h) {

@@ -261,8 +261,12 @@ __global__ void __launch_bounds__(kForceBlock)
         atomicAdd(&counts[4], (unsigned long long)nChunk);
       }
     } else if (valid) {
-      if (query) queryAcc[i] = make_float2(ax, ay);
-      else S.acc[i] = make_float2(ax, ay);
+      if (query) {
+        queryAcc[i] = make_float2(ax, ay);
+      } else {
+        add_attractor<kExact>(S.attr, x, y, ax, ay);
+        S.acc[i] = make_float2(ax, ay);
+      }
     }
   }
 }

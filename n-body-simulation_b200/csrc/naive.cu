@@ -122,8 +122,11 @@ __global__ void __launch_bounds__(kNaiveThreads)
     __syncthreads();
   }
 #pragma unroll
-  for (int t = 0; t < kNaiveTargets; ++t)
-    if (idx[t] < S.n) S.acc[idx[t]] = make_float2(ax[t], ay[t]);
+  for (int t = 0; t < kNaiveTargets; ++t) {
+    if (idx[t] >= S.n) continue;
+    add_attractor<kExact>(S.attr, x[t], y[t], ax[t], ay[t]);
+    S.acc[idx[t]] = make_float2(ax[t], ay[t]);
+  }
 }
 
 // The naive step's stand-in for the Morton gather: the same buffer swap,

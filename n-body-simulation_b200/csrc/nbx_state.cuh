@@ -108,6 +108,36 @@ struct DevState {
   int4 *tB;   // {next (preorder, global), start, end, isLeaf}
   float4 *tM; // {Ixx, Iyy, Ixy, size} for the learned correction
   float2 *tC; // square centre, for the learned correction
+
+  // attractor: [0] = {x, y, mass, softening}, [1].x = active (0 or 1);
+  // device-resident so it can move between steps of a captured graph
+  float4 *attr;
 };
+
+// The viewer's attractor pull (attractorKernel, src/cuda/CudaSimulation.cu
+// :14-31): acc += d * m / (sqrt(|d|^2 + 1e-12) (|d|^2 + soft^2)), d = a - p,
+// added after the gravitational sum.  kExact: IEEE reciprocal square root
+// and division, no contraction; otherwise the hardware rsqrt, an IEEE
+// division and fused multiply-adds, as the reference's kernel compiles.
+template <bool kExact>
+__device__ __forceinline__ void add_attractor(const float4 *attr, float px, float py,
+                                              float &ax, float &ay) {
+  if (attr[1].x == 0.0f) return;
+  const float4 a = attr[0];
+  if (kExact) {
+    const float dx = __fsub_rn(a.x, px), dy = __fsub_rn(a.y, py);
+    const float dSq = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+    const float f = __fdiv_rn(__fmul_rn(a.z, __frcp_rn(__fsqrt_rn(__fadd_rn(dSq, 1e-12f)))),
+                              __fadd_rn(dSq, __fmul_rn(a.w, a.w)));
+    ax = __fadd_rn(ax, __fmul_rn(dx, f));
+    ay = __fadd_rn(ay, __fmul_rn(dy, f));
+  } else {
+    const float dx = a.x - px, dy = a.y - py;
+    const float dSq = dx * dx + dy * dy;
+    const float f = __fdiv_rn(a.z * rsqrtf(dSq + 1e-12f), dSq + a.w * a.w);
+    ax = fmaf(dx, f, ax);
+    ay = fmaf(dy, f, ay);
+  }
+}
 
 } // namespace nbx

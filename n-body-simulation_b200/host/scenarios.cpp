@@ -97,17 +97,8 @@ extern "C" int nbx_two_discs(uint32_t n, uint32_t seed, float approach,
 }
 
 extern "C" int nbx_cold_square(uint32_t n, uint32_t seed, nbx_body *out) {
-  if (!out && n) return NBX_ERR_ARG;
-  std::mt19937 rng(seed);
-  const float h = 3.0f * std::sqrt(static_cast<float>(n));
-  std::uniform_real_distribution<float> coord(-h, h);
-  Rec *o = reinterpret_cast<Rec *>(out);
-  for (uint32_t i = 0; i < n; ++i) {
-    const float x = coord(rng);
-    const float y = coord(rng);
-    o[i] = Rec{{x, y}, {0.0f, 0.0f}, {0.0f, 0.0f}, 1.0f, 1.0f, i};
-  }
-  return NBX_OK;
+  // the viewer's ColdSquare, built with the viewer's flags (edits.cpp)
+  return nbx_make_scenario(NBX_SCENARIO_COLD_SQUARE, n, seed, out);
 }
 
 // Instance sizes of the batched ensemble: N_i = round(exp(U(ln lo, ln hi)))

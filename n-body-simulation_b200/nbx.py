@@ -37,7 +37,10 @@ EXPORTS = (
     "nbx_mlp_get_params", "nbx_mlp_init", "nbx_mlp_harvest", "nbx_mlp_train",
     "nbx_mlp_gradient", "nbx_mlp_eval", "nbx_ensemble_sizes", "nbx_autotune",
     "nbx_direct_fp64_noalloc", "nbx_step_timed", "nbx_force_times",
+    "nbx_make_scenario", "nbx_renumber", "nbx_add_heavy_body", "nbx_add_cluster",
+    "nbx_set_attractor", "nbx_reset",
 )
+SCENARIOS = {"disc": 0, "two_galaxies": 1, "cold_square": 2}
 MLP_PARAMS = 1442
 MLP_ROW = 12
 
@@ -92,6 +95,9 @@ def lib() -> C.CDLL:
         "nbx_step": [vp, C.c_uint32],
         "nbx_step_timed": [vp, C.c_uint32],
         "nbx_force_times": [vp, vp, C.c_uint32],
+        "nbx_make_scenario": [C.c_int, C.c_uint32, C.c_uint32, vp],
+        "nbx_set_attractor": [vp, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float],
+        "nbx_reset": [vp, vp, C.c_size_t],
         "nbx_sync": [vp],
         "nbx_phase": [vp, C.c_int],
         "nbx_get_morton": [vp, C.c_uint32, u64p, u32p, C.c_size_t],
@@ -132,6 +138,13 @@ def lib() -> C.CDLL:
         f = getattr(L, name)
         f.argtypes = args
         f.restype = C.c_int
+    L.nbx_renumber.argtypes = [vp, C.c_size_t]
+    L.nbx_renumber.restype = None
+    L.nbx_add_heavy_body.argtypes = [vp, C.c_size_t, C.c_float, C.c_float, C.c_float]
+    L.nbx_add_heavy_body.restype = C.c_size_t
+    L.nbx_add_cluster.argtypes = [vp, C.c_size_t, C.c_float, C.c_float, C.c_float,
+                                  C.c_float, C.c_size_t, C.c_uint32]
+    L.nbx_add_cluster.restype = C.c_size_t
     L.nbx_last_error.restype = C.c_char_p
     L.nbx_version.restype = C.c_char_p
     _lib = L
@@ -168,6 +181,35 @@ def cold_square(n: int, seed: int = 0) -> np.ndarray:
     b = np.zeros(n, BODY_DTYPE)
     _check(None, lib().nbx_cold_square(n, seed, b))
     return b
+
+
+def make_scenario(kind: str, n: int, seed: int = 0) -> np.ndarray:
+    """The viewer's makeScenario (viewer/Scenarios.cpp:28-62)."""
+    b = np.zeros(n, BODY_DTYPE)
+    _check(None, lib().nbx_make_scenario(SCENARIOS[kind], n, seed, b.ctypes.data))
+    return b
+
+
+def add_heavy_body(bodies: np.ndarray, x: float, y: float, mass: float) -> np.ndarray:
+    """addHeavyBody (viewer/Scenarios.cpp:64-70) on a copy."""
+    out = np.zeros(len(bodies) + 1, BODY_DTYPE)
+    out[:len(bodies)] = bodies
+    lib().nbx_add_heavy_body(out.ctypes.data, len(bodies), x, y, mass)
+    return out
+
+
+def add_cluster(bodies: np.ndarray, x, y, vx, vy, count: int, seed: int) -> np.ndarray:
+    """addCluster (viewer/Scenarios.cpp:72-86) on a copy."""
+    out = np.zeros(len(bodies) + count, BODY_DTYPE)
+    out[:len(bodies)] = bodies
+    lib().nbx_add_cluster(out.ctypes.data, len(bodies), x, y, vx, vy, count, seed)
+    return out
+
+
+def renumber(bodies: np.ndarray) -> np.ndarray:
+    out = np.ascontiguousarray(bodies.copy())
+    lib().nbx_renumber(out.ctypes.data, len(out))
+    return out
 
 
 def ensemble_sizes(count: int, lo: int = 2000, hi: int = 200000) -> np.ndarray:
@@ -251,6 +293,18 @@ class Handle:
 
     def step(self, steps: int = 1):
         self._c(lib().nbx_step(self.h, steps))
+
+    def set_attractor(self, active: bool, x=0.0, y=0.0, mass=1e6, softening=50.0):
+        """The viewer's attractor (CudaSimulation.cuh:9-15)."""
+        self._c(lib().nbx_set_attractor(self.h, int(active), x, y, mass, softening))
+
+    def reset(self, bodies: np.ndarray):
+        """CudaSimulation::reset: replace every body (any count)."""
+        b = np.ascontiguousarray(bodies, BODY_DTYPE)
+        self._c(lib().nbx_reset(self.h, b.ctypes.data, len(b)))
+        self.sizes = np.array([len(b)], np.uint32)
+        self.n = len(b)
+        self.starts = np.zeros(1, np.int64)
 
     def step_timed(self, steps: int):
         """Like step(), recording each step's force-pass duration on the
