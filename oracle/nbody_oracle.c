@@ -916,3 +916,14 @@ int orc_naive_step(size_t n, orc_body *b, float dt, float epsilon, int collision
   free(x);
   return 0;
 }
+
+void orc_attractor(size_t n, const float *x, const float *y, float axp, float ayp,
+                   float mass, float softening, float *ax, float *ay) {
+  for (size_t i = 0; i < n; ++i) {
+    const float dx = axp - x[i], dy = ayp - y[i];
+    const float dSq = dx * dx + dy * dy;
+    const float f = (mass * (1.0f / sqrtf(dSq + 1e-12f))) / (dSq + softening * softening);
+    ax[i] = ax[i] + dx * f;
+    ay[i] = ay[i] + dy * f;
+  }
+}

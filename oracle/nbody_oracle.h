@@ -112,6 +112,13 @@ void orc_naive_forces(size_t n, const float *x, const float *y, const float *m,
  * -> naive attract; bodies keep their order.  Returns 0, or -1. */
 int orc_naive_step(size_t n, orc_body *b, float dt, float epsilon, int collisions);
 
+/* The viewer's attractor pull (attractorKernel,
+ * src/cuda/CudaSimulation.cu:14-31) added to ax/ay in IEEE single
+ * precision: d = a - p, f = (m * (1/sqrt(|d|^2 + 1e-12))) / (|d|^2 + s^2),
+ * acc += d * f. */
+void orc_attractor(size_t n, const float *x, const float *y, float axp, float ayp,
+                   float mass, float softening, float *ax, float *ay);
+
 /* FP64 direct sum with the tree's force law for the given targets
  * (exactTreeLawForces, src/cuda/CheckCuda.cu:453-475; eps generalised). */
 void orc_direct_fp64(size_t n, const float *x, const float *y, const float *m,

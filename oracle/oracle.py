@@ -111,6 +111,8 @@ class Oracle:
         L.orc_naive_step.argtypes = [C.c_size_t, _bodyp, C.c_float, C.c_float,
                                      C.c_int]
         L.orc_naive_step.restype = C.c_int
+        L.orc_attractor.argtypes = [C.c_size_t, _f32p, _f32p, C.c_float, C.c_float,
+                                    C.c_float, C.c_float, _f32p, _f32p]
         L.orc_direct_fp64.argtypes = [C.c_size_t, _f32p, _f32p, _f32p,
                                       C.c_double, C.c_size_t, _u32p, _f64p,
                                       _f64p]
@@ -243,6 +245,15 @@ class Oracle:
             if self.L.orc_naive_step(len(b), b, dt, eps, int(collisions)) != 0:
                 raise RuntimeError("oracle naive step failed")
         return b
+
+    def attractor(self, x, y, ax, ay, at, mass=1e6, softening=50.0):
+        """attractorKernel (CudaSimulation.cu:14-31), IEEE; returns new ax, ay."""
+        ax = np.array(ax, np.float32, copy=True)
+        ay = np.array(ay, np.float32, copy=True)
+        self.L.orc_attractor(len(ax), np.ascontiguousarray(x, np.float32),
+                             np.ascontiguousarray(y, np.float32), at[0], at[1],
+                             mass, softening, ax, ay)
+        return ax, ay
 
     def direct_fp64(self, b: np.ndarray, eps, targets):
         targets = np.ascontiguousarray(targets, np.uint32)
