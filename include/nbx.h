@@ -207,7 +207,22 @@ int nbx_nbs2_open(const char *path, uint32_t n, uint32_t total_steps,
 /* One frame from body records in id order (nbx_download_bodies with
  * id_order = 1). */
 int nbx_nbs2_write_frame(nbx_nbs2 *f, const nbx_body *bodies_by_id);
+/* One frame already in record layout: {x, y, vx, vy} per body, id order. */
+int nbx_nbs2_write_packed(nbx_nbs2 *f, const float *xyvv_by_id, uint32_t n);
 int nbx_nbs2_close(nbx_nbs2 *f);
+
+/* Device-path frame output for a single-instance handle (MainCuda.cu:90-105
+ * downloads the bodies and scatters them by id on the host).  Records the
+ * current state as the next frame of f: an id-order scatter of
+ * {x, y, vx, vy} on the handle's stream, a copy into pinned host memory on a
+ * second stream, and a writer thread that appends it to f -- so the copy and
+ * the file write overlap the steps enqueued after the call.  Frames are
+ * written in call order; two frames can be in flight, a third call waits for
+ * the oldest to be written.  Do not write to f by other calls until
+ * nbx_nbs2_flush has returned.  No counterpart in the reference. */
+int nbx_nbs2_record(nbx_handle *h, nbx_nbs2 *f);
+/* Waits until every recorded frame is written; returns the first error. */
+int nbx_nbs2_flush(nbx_handle *h);
 
 /* --- FP64 checks --- */
 

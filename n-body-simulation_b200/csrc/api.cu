@@ -6,6 +6,10 @@
 
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -71,6 +75,15 @@ __global__ void k_unpack(const nbx_body *__restrict__ in, uint32_t n,
   }
 }
 
+// NBS2 frame record in id order: {x, y, vx, vy} = the body's pv record.
+__global__ void k_frame_scatter(const float4 *__restrict__ pv,
+                                const uint32_t *__restrict__ id, uint32_t n,
+                                float4 *__restrict__ frame) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x)
+    frame[id[i]] = pv[i];
+}
+
 // Body records; id_order scatters body i to instance_start + id.
 __global__ void k_pack(const float4 *__restrict__ pv, const float2 *__restrict__ acc,
                        const float2 *__restrict__ mr, const uint32_t *__restrict__ id,
@@ -122,6 +135,51 @@ template <typename T> struct DevBuf {
 
 } // namespace
 
+
+// Device-path frame output: an id-order scatter on the handle's stream into
+// one of two device frames, a copy into a pinned slot on a second stream
+// (overlapping the following steps), and a writer thread that appends the
+// slot to the file once its copy has completed.
+struct FrameWriter {
+  int device = 0;
+  uint32_t n = 0;
+  cudaStream_t copy = nullptr;
+  float4 *dFrame[2] = {nullptr, nullptr};
+  float *hSlot[2] = {nullptr, nullptr};
+  cudaEvent_t scattered[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
+  int next = 0;
+  std::thread th;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<std::pair<int, nbx_nbs2 *>> queue; // (slot, file), in call order
+  bool busy[2] = {false, false};                // slot copied or being written
+  bool stop = false;
+  int err = NBX_OK;
+
+  void run() {
+    cudaSetDevice(device);
+    for (;;) {
+      std::pair<int, nbx_nbs2 *> job;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return stop || !queue.empty(); });
+        if (queue.empty()) return; // stop with nothing pending
+        job = queue.front();
+      }
+      const int sl = job.first;
+      int rc = cudaEventSynchronize(copied[sl]) == cudaSuccess ? NBX_OK : NBX_ERR_CUDA;
+      if (rc == NBX_OK) rc = nbx_nbs2_write_packed(job.second, hSlot[sl], n);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        if (rc != NBX_OK && err == NBX_OK) err = rc;
+        queue.pop_front();
+        busy[sl] = false;
+      }
+      cv.notify_all();
+    }
+  }
+};
+
 struct nbx_handle {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -168,6 +226,7 @@ struct nbx_handle {
   // attractor (CudaSimulation.cuh:9-15 defaults): {x, y, mass, softening},
   // {active, 0, 0, 0}; mirrored into S.attr
   float attrHost[8] = {0.0f, 0.0f, 1e6f, 50.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  FrameWriter *frames = nullptr; // created by the first nbx_nbs2_record
 
   DevState state() const {
     DevState S = base;
@@ -538,6 +597,9 @@ int nbx_params_default(nbx_params *p) {
   return NBX_OK;
 }
 
+static int frames_flush(nbx_handle *h);
+static void frames_destroy(nbx_handle *h);
+
 int nbx_create(const nbx_params *p, uint32_t num, const uint32_t *sizes,
                nbx_handle **out) {
   if (!out || num == 0 || !sizes || num > 65535) return NBX_ERR_ARG;
@@ -579,6 +641,7 @@ int nbx_destroy(nbx_handle *h) {
   if (!h) return NBX_ERR_ARG;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  frames_destroy(h);
   destroy_graphs(h);
   for (cudaEvent_t ev : h->forceEv) cudaEventDestroy(ev);
   for (cudaEvent_t ev : h->forceMark)
@@ -670,12 +733,10 @@ int nbx_upload_bodies(nbx_handle *h, const nbx_body *bodies, size_t n) {
   return NBX_OK;
 }
 
-int nbx_download_bodies(nbx_handle *h, nbx_body *bodies, size_t n, int idOrder) {
-  if (!h || (!bodies && n) || n != h->n) return h ? fail(h, NBX_ERR_ARG, "body count mismatch") : NBX_ERR_ARG;
-  cudaSetDevice(h->device);
-  if (idOrder && !h->idsChecked) {
-    // ids must be a permutation of 0..size-1 in every instance; checked on
-    // the device once per upload (steps only permute bodies)
+// ids must be a permutation of 0..size-1 in every instance for id-order
+// output; checked on the device once per upload (steps only permute bodies).
+static int ensure_id_permutation(nbx_handle *h) {
+  if (!h->idsChecked) {
     const DevState S0 = h->state();
     uint32_t *seen = S0.splitCount, *bad = S0.counters + 8;
     NBX_CUDA(h, cudaMemsetAsync(seen, 0, 4ull * h->n, h->stream));
@@ -688,8 +749,18 @@ int nbx_download_bodies(nbx_handle *h, nbx_body *bodies, size_t n, int idOrder) 
     h->idsPermutation = b == 0;
     h->idsChecked = true;
   }
-  if (idOrder && !h->idsPermutation)
+  if (!h->idsPermutation)
     return fail(h, NBX_ERR_ARG, "ids are not a permutation of 0..size-1 per instance");
+  return NBX_OK;
+}
+
+int nbx_download_bodies(nbx_handle *h, nbx_body *bodies, size_t n, int idOrder) {
+  if (!h || (!bodies && n) || n != h->n) return h ? fail(h, NBX_ERR_ARG, "body count mismatch") : NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (idOrder) {
+    const int rc = ensure_id_permutation(h);
+    if (rc != NBX_OK) return rc;
+  }
   if (n == 0) return NBX_OK;
   const DevState S = h->state();
   k_pack<<<std::min<uint32_t>((h->n + 255) / 256, 4096), 256, 0, h->stream>>>(
@@ -769,6 +840,94 @@ int nbx_force_times(nbx_handle *h, float *ms, uint32_t count) {
   return check_status(h);
 }
 
+// Waits for every recorded frame to be written; returns the first error.
+static int frames_flush(nbx_handle *h) {
+  FrameWriter *w = h->frames;
+  if (!w) return NBX_OK;
+  std::unique_lock<std::mutex> lk(w->mu);
+  w->cv.wait(lk, [&] { return w->queue.empty(); });
+  const int rc = w->err;
+  w->err = NBX_OK;
+  return rc;
+}
+
+static void frames_destroy(nbx_handle *h) {
+  FrameWriter *w = h->frames;
+  if (!w) return;
+  {
+    std::lock_guard<std::mutex> lk(w->mu);
+    w->stop = true;
+  }
+  w->cv.notify_all();
+  if (w->th.joinable()) w->th.join(); // drains the queue first
+  for (int k = 0; k < 2; ++k) {
+    if (w->dFrame[k]) cudaFree(w->dFrame[k]);
+    if (w->hSlot[k]) cudaFreeHost(w->hSlot[k]);
+    if (w->scattered[k]) cudaEventDestroy(w->scattered[k]);
+    if (w->copied[k]) cudaEventDestroy(w->copied[k]);
+  }
+  if (w->copy) cudaStreamDestroy(w->copy);
+  delete w;
+  h->frames = nullptr;
+}
+
+int nbx_nbs2_record(nbx_handle *h, nbx_nbs2 *f) {
+  if (!h || !f) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (h->nseg != 1) return fail(h, NBX_ERR_ARG, "NBS2 frames hold one simulation");
+  if (!h->uploaded) return fail(h, NBX_ERR_STATE, "no bodies uploaded");
+  int rc = ensure_id_permutation(h);
+  if (rc != NBX_OK) return rc;
+  if (!h->frames) {
+    FrameWriter *w = new (std::nothrow) FrameWriter();
+    if (!w) return NBX_ERR_NOMEM;
+    h->frames = w;
+    w->device = h->device;
+    w->n = h->n;
+    NBX_CUDA(h, cudaStreamCreateWithFlags(&w->copy, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) {
+      NBX_CUDA(h, cudaMalloc(&w->dFrame[k], std::max<size_t>(w->n, 1) * sizeof(float4)));
+      NBX_CUDA(h, cudaMallocHost(&w->hSlot[k], std::max<size_t>(w->n, 1) * sizeof(float4)));
+      NBX_CUDA(h, cudaEventCreateWithFlags(&w->scattered[k], cudaEventDisableTiming));
+      NBX_CUDA(h, cudaEventCreateWithFlags(&w->copied[k], cudaEventDisableTiming));
+    }
+    w->th = std::thread([w] { w->run(); });
+  }
+  FrameWriter *w = h->frames;
+  const int sl = w->next;
+  {
+    // the slot's previous frame must be written before it is reused
+    std::unique_lock<std::mutex> lk(w->mu);
+    w->cv.wait(lk, [&] { return !w->busy[sl]; });
+    w->busy[sl] = true;
+  }
+  const DevState S = h->state();
+  if (w->n) {
+    k_frame_scatter<<<std::min<uint32_t>((w->n + 255) / 256, 4096), 256, 0, h->stream>>>(
+        S.pv, S.id, w->n, w->dFrame[sl]);
+    NBX_CUDA(h, cudaGetLastError());
+  }
+  NBX_CUDA(h, cudaEventRecord(w->scattered[sl], h->stream));
+  NBX_CUDA(h, cudaStreamWaitEvent(w->copy, w->scattered[sl], 0));
+  NBX_CUDA(h, cudaMemcpyAsync(w->hSlot[sl], w->dFrame[sl], (size_t)w->n * sizeof(float4),
+                              cudaMemcpyDeviceToHost, w->copy));
+  NBX_CUDA(h, cudaEventRecord(w->copied[sl], w->copy));
+  {
+    std::lock_guard<std::mutex> lk(w->mu);
+    w->queue.emplace_back(sl, f);
+  }
+  w->cv.notify_all();
+  w->next ^= 1;
+  return NBX_OK;
+}
+
+int nbx_nbs2_flush(nbx_handle *h) {
+  if (!h) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  const int rc = frames_flush(h);
+  return rc == NBX_OK ? NBX_OK : fail(h, rc, "writing a recorded NBS2 frame failed");
+}
+
 int nbx_set_attractor(nbx_handle *h, int active, float x, float y, float mass,
                       float softening) {
   if (!h) return NBX_ERR_ARG;
@@ -789,6 +948,10 @@ int nbx_reset(nbx_handle *h, const nbx_body *bodies, size_t n) {
     return fail(h, NBX_ERR_ARG, "nbx_reset replaces the bodies of a single-instance handle");
   cudaSetDevice(h->device);
   NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  // pending frames are written first; the writer is rebuilt for the new size
+  const int frc = frames_flush(h);
+  frames_destroy(h);
+  if (frc != NBX_OK) return fail(h, frc, "writing a recorded NBS2 frame failed");
   // keep the network parameters across the reallocation (optimizer
   // moments start again)
   std::vector<float> mlp;

@@ -19,6 +19,19 @@ bool put(std::FILE *f, const void *p, size_t bytes) {
 }
 } // namespace
 
+// Appends a frame already in NBS2 record layout ({x, y, vx, vy} x n, id
+// order) and bumps completed_frames.
+static int append_frame(nbx_nbs2 *w, const float *rec) {
+  if (!put(w->f, rec, 16ull * w->n)) return NBX_ERR_ARG;
+  ++w->completed;
+  const long end = std::ftell(w->f);
+  if (std::fseek(w->f, kCompletedOffset, SEEK_SET) != 0 ||
+      !put(w->f, &w->completed, 4) || std::fseek(w->f, end, SEEK_SET) != 0)
+    return NBX_ERR_ARG;
+  std::fflush(w->f);
+  return NBX_OK;
+}
+
 extern "C" int nbx_nbs2_open(const char *path, uint32_t n, uint32_t steps,
                              uint32_t every, float dt, const float *mass,
                              const float *radius, nbx_nbs2 **out) {
@@ -51,15 +64,12 @@ extern "C" int nbx_nbs2_write_frame(nbx_nbs2 *w, const nbx_body *b) {
     w->frame[4 * i + 2] = b[i].vel_x;
     w->frame[4 * i + 3] = b[i].vel_y;
   }
-  if (!put(w->f, w->frame.data(), 16ull * w->n)) return NBX_ERR_ARG;
-  // bump completed_frames in place, then return to the end
-  ++w->completed;
-  const long end = std::ftell(w->f);
-  if (std::fseek(w->f, kCompletedOffset, SEEK_SET) != 0 ||
-      !put(w->f, &w->completed, 4) || std::fseek(w->f, end, SEEK_SET) != 0)
-    return NBX_ERR_ARG;
-  std::fflush(w->f);
-  return NBX_OK;
+  return append_frame(w, w->frame.data());
+}
+
+extern "C" int nbx_nbs2_write_packed(nbx_nbs2 *w, const float *xyvv, uint32_t n) {
+  if (!w || n != w->n || (n && !xyvv)) return NBX_ERR_ARG;
+  return append_frame(w, xyvv);
 }
 
 extern "C" int nbx_nbs2_close(nbx_nbs2 *w) {

@@ -120,11 +120,13 @@ int main(int argc, char **argv) {
                      .count();
     step += chunk;
     if (writeOutput && step % every == 0) {
-      if (nbx_download_bodies(h, bodies.data(), n, 1) != NBX_OK) return fail("download", h);
-      if (nbx_nbs2_write_frame(out, bodies.data()) != NBX_OK) return fail("write", h);
+      // device path: id-order scatter on the GPU, copy and file write
+      // overlapped with the following steps
+      if (nbx_nbs2_record(h, out) != NBX_OK) return fail("record frame", h);
       ++completed;
     }
   }
+  if (out && nbx_nbs2_flush(h) != NBX_OK) return fail("write", h);
   const double loopMs = std::chrono::duration<double, std::milli>(
                             std::chrono::steady_clock::now() - loopStart)
                             .count();

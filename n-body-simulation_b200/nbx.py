@@ -38,7 +38,8 @@ EXPORTS = (
     "nbx_mlp_gradient", "nbx_mlp_eval", "nbx_ensemble_sizes", "nbx_autotune",
     "nbx_direct_fp64_noalloc", "nbx_step_timed", "nbx_force_times",
     "nbx_make_scenario", "nbx_renumber", "nbx_add_heavy_body", "nbx_add_cluster",
-    "nbx_set_attractor", "nbx_reset",
+    "nbx_set_attractor", "nbx_reset", "nbx_nbs2_record", "nbx_nbs2_flush",
+    "nbx_nbs2_open", "nbx_nbs2_write_packed", "nbx_nbs2_close",
 )
 SCENARIOS = {"disc": 0, "two_galaxies": 1, "cold_square": 2}
 MLP_PARAMS = 1442
@@ -145,6 +146,11 @@ def lib() -> C.CDLL:
     L.nbx_add_cluster.argtypes = [vp, C.c_size_t, C.c_float, C.c_float, C.c_float,
                                   C.c_float, C.c_size_t, C.c_uint32]
     L.nbx_add_cluster.restype = C.c_size_t
+    L.nbx_nbs2_open.argtypes = [C.c_char_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                C.c_float, vp, vp, C.POINTER(vp)]
+    L.nbx_nbs2_record.argtypes = [vp, vp]
+    L.nbx_nbs2_flush.argtypes = [vp]
+    L.nbx_nbs2_close.argtypes = [vp]
     L.nbx_last_error.restype = C.c_char_p
     L.nbx_version.restype = C.c_char_p
     _lib = L
@@ -181,6 +187,24 @@ def cold_square(n: int, seed: int = 0) -> np.ndarray:
     b = np.zeros(n, BODY_DTYPE)
     _check(None, lib().nbx_cold_square(n, seed, b))
     return b
+
+
+class Nbs2Writer:
+    """An NBS2 output file (src/Main.cpp:13-49): header, mass and radius by
+    id, then frames written by Handle.nbs2_record or write_frame."""
+
+    def __init__(self, path, n, total_steps, every, dt, mass_by_id, radius_by_id):
+        m = np.ascontiguousarray(mass_by_id, np.float32)
+        r = np.ascontiguousarray(radius_by_id, np.float32)
+        f = C.c_void_p()
+        _check(None, lib().nbx_nbs2_open(str(path).encode(), n, total_steps, every,
+                                         dt, m.ctypes.data, r.ctypes.data, C.byref(f)))
+        self.f = f
+
+    def close(self):
+        if self.f:
+            _check(None, lib().nbx_nbs2_close(self.f))
+            self.f = None
 
 
 def make_scenario(kind: str, n: int, seed: int = 0) -> np.ndarray:
@@ -293,6 +317,13 @@ class Handle:
 
     def step(self, steps: int = 1):
         self._c(lib().nbx_step(self.h, steps))
+
+    def nbs2_record(self, writer: "Nbs2Writer"):
+        """Records the current state as writer's next frame (device path)."""
+        self._c(lib().nbx_nbs2_record(self.h, writer.f))
+
+    def nbs2_flush(self):
+        self._c(lib().nbx_nbs2_flush(self.h))
 
     def set_attractor(self, active: bool, x=0.0, y=0.0, mass=1e6, softening=50.0):
         """The viewer's attractor (CudaSimulation.cuh:9-15)."""
