@@ -143,6 +143,33 @@ int nbx_set_attractor(nbx_handle *h, int active, float x, float y, float mass,
  * Parameters, the attractor and loaded network parameters are kept. */
 int nbx_reset(nbx_handle *h, const nbx_body *bodies, size_t n);
 
+/* Headless splat renderer: the viewer's point-sprite drawing
+ * (viewer/Renderer.cpp:8-52 shaders, 113-147 blending) rasterised by CUDA
+ * into a float RGBA image, no graphics API.  Camera: screen = (world -
+ * centre) * scale pixels from the image centre, y up (Renderer.h:5-10). */
+typedef struct nbx_camera {
+  float center_x, center_y;
+  float scale; /* pixels per world unit */
+} nbx_camera;
+typedef struct nbx_draw {   /* DrawSettings (Renderer.h:14-20) */
+  int32_t mode;             /* 0: speed colour ramp, composited over in draw
+                               order; 1: glow, additive (default) */
+  float point_scale;        /* multiplies each body's true size (1) */
+  float min_point_px;       /* smallest drawn point; smaller ones fade (1.5) */
+  float brightness;         /* (0.6) */
+  float speed_max;          /* speed at the top of the colour ramp (60) */
+} nbx_draw;
+int nbx_draw_default(nbx_draw *d);
+/* Renders the handle's bodies in their current array order (the order the
+ * viewer draws) into rgba[height][width][4] (host memory, premultiplied,
+ * row 0 at the bottom, cleared to (0, 0, 0.02, 1)); rgba may be NULL.
+ * stats (may be NULL) receives the viewer's BodyStats {centre-of-mass x,
+ * y, max speed} (Interop.cu:14-45, 80-104).  width, height <= 16384. */
+int nbx_render(nbx_handle *h, const nbx_camera *cam, const nbx_draw *draw,
+               uint32_t width, uint32_t height, float *rgba, float *stats);
+/* BodyStats alone, for a follow-the-centre camera. */
+int nbx_body_stats(nbx_handle *h, float *stats);
+
 /* nbx_step with the duration of each step's force pass recorded by CUDA
  * events on the handle's stream, around the force launch inside the step's
  * graph (the same kernels as nbx_step, plus two event records per step).

@@ -27,6 +27,16 @@ void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
                   SortScratch &sort);
 void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
                    const MlpDev *mlp, float band, int corr);
+void render_vertices(cudaStream_t s, const float4 *pv, const float2 *mr, uint32_t n,
+                     const RenderParams &P, float4 *v0, float4 *v1, uint32_t *tiles,
+                     double4 *partial, unsigned long long *total, float *stats);
+uint32_t render_vertex_blocks(uint32_t n);
+void render_emit(cudaStream_t s, const float4 *v0, const uint32_t *off, uint32_t n,
+                 const RenderParams &P, uint64_t *keys, uint32_t *vals);
+void render_composite(cudaStream_t s, const float4 *v0, const float4 *v1,
+                      const uint64_t *keys, const uint32_t *bodies, const uint32_t *count,
+                      uint32_t maxEntries, uint32_t *first, uint32_t *last,
+                      const RenderParams &P, float4 *image);
 DevState launch_naive_gather(cudaStream_t s, const DevState &S);
 void launch_naive_forces(cudaStream_t s, const DevState &S, bool exact);
 void mlp_harvest(cudaStream_t s, const DevState &S, const uint32_t *targets,
@@ -227,6 +237,17 @@ struct nbx_handle {
   // {active, 0, 0, 0}; mirrored into S.attr
   float attrHost[8] = {0.0f, 0.0f, 1e6f, 50.0f, 0.0f, 0.0f, 0.0f, 0.0f};
   FrameWriter *frames = nullptr; // created by the first nbx_nbs2_record
+  // splat renderer buffers, grown on demand
+  struct {
+    uint32_t bodies = 0, entries = 0, tiles = 0;
+    size_t pixels = 0;
+    float4 *v0 = nullptr, *v1 = nullptr, *image = nullptr;
+    uint32_t *count = nullptr, *off = nullptr, *first = nullptr, *last = nullptr;
+    double4 *partial = nullptr;
+    unsigned long long *total = nullptr;
+    float *stats = nullptr;
+    SortScratch sort;
+  } rs;
 
   DevState state() const {
     DevState S = base;
@@ -574,6 +595,13 @@ bool valid_params(const nbx_params *p) {
 
 } // namespace
 
+// Reallocates p for count elements (contents are not kept).
+template <typename T> static cudaError_t grow(T *&p, size_t count) {
+  if (p) cudaFree(p);
+  p = nullptr;
+  return cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+}
+
 extern "C" {
 
 const char *nbx_version(void) { return "nbx 0.1 (sm_100a)"; }
@@ -599,6 +627,7 @@ int nbx_params_default(nbx_params *p) {
 
 static int frames_flush(nbx_handle *h);
 static void frames_destroy(nbx_handle *h);
+static void render_free(nbx_handle *h);
 
 int nbx_create(const nbx_params *p, uint32_t num, const uint32_t *sizes,
                nbx_handle **out) {
@@ -642,6 +671,7 @@ int nbx_destroy(nbx_handle *h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   frames_destroy(h);
+  render_free(h);
   destroy_graphs(h);
   for (cudaEvent_t ev : h->forceEv) cudaEventDestroy(ev);
   for (cudaEvent_t ev : h->forceMark)
@@ -928,6 +958,162 @@ int nbx_nbs2_flush(nbx_handle *h) {
   return rc == NBX_OK ? NBX_OK : fail(h, rc, "writing a recorded NBS2 frame failed");
 }
 
+static void render_free(nbx_handle *h) {
+  auto &r = h->rs;
+  void *ptrs[] = {r.v0, r.v1, r.image, r.count, r.off, r.first, r.last, r.partial,
+                  r.total, r.stats, r.sort.keys[0], r.sort.keys[1], r.sort.vals[0],
+                  r.sort.vals[1], r.sort.hist, r.sort.status, r.sort.tileCounter};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  r = {};
+}
+
+// Vertices and statistics of the current state for image P; on return the
+// stats (3 floats) are on the device and the entry total is known.
+static int render_prepare(nbx_handle *h, const RenderParams &P, unsigned long long *entries) {
+  auto &r = h->rs;
+  const uint32_t n = h->n;
+  if (r.bodies < n || !r.v0) {
+    NBX_CUDA(h, grow(r.v0, n));
+    NBX_CUDA(h, grow(r.v1, n));
+    NBX_CUDA(h, grow(r.count, n));
+    NBX_CUDA(h, grow(r.off, n));
+    NBX_CUDA(h, grow(r.partial, render_vertex_blocks(n)));
+    if (!r.total) NBX_CUDA(h, cudaMalloc(&r.total, 2 * sizeof(unsigned long long)));
+    if (!r.stats) NBX_CUDA(h, cudaMalloc(&r.stats, 4 * sizeof(float)));
+    r.bodies = n;
+  }
+  const DevState S = h->state();
+  render_vertices(h->stream, S.pv, S.mr, n, P, r.v0, r.v1, r.count, r.partial, r.total,
+                  r.stats);
+  NBX_CUDA(h, cudaGetLastError());
+  NBX_CUDA(h, cudaMemcpyAsync(entries, r.total, sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  return NBX_OK;
+}
+
+static int render_params(const nbx_camera *cam, const nbx_draw *d, uint32_t width,
+                         uint32_t height, RenderParams &P) {
+  if (!cam || !d || width == 0 || height == 0 || width > 16384 || height > 16384 ||
+      (d->mode != 0 && d->mode != 1) || !(d->min_point_px > 0.0f) || !(d->speed_max > 0.0f))
+    return NBX_ERR_ARG;
+  P.camX = cam->center_x;
+  P.camY = cam->center_y;
+  P.scale = cam->scale;
+  P.halfW = (float)width * 0.5f;
+  P.halfH = (float)height * 0.5f;
+  P.width = width;
+  P.height = height;
+  P.tilesX = (width + 15) / 16;
+  P.tilesY = (height + 15) / 16;
+  P.mode = d->mode;
+  P.pointScale = d->point_scale;
+  P.minPoint = d->min_point_px;
+  P.brightness = d->brightness;
+  P.speedMax = d->speed_max;
+  return NBX_OK;
+}
+
+int nbx_draw_default(nbx_draw *d) {
+  if (!d) return NBX_ERR_ARG;
+  d->mode = 1; // glow
+  d->point_scale = 1.0f;
+  d->min_point_px = 1.5f;
+  d->brightness = 0.6f;
+  d->speed_max = 60.0f;
+  return NBX_OK;
+}
+
+int nbx_body_stats(nbx_handle *h, float *stats) {
+  if (!h || !stats) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!h->uploaded) return fail(h, NBX_ERR_STATE, "no bodies uploaded");
+  if (h->n == 0) {
+    stats[0] = stats[1] = 0.0f;
+    stats[2] = 1.0f;
+    return NBX_OK;
+  }
+  const nbx_camera cam = {0.0f, 0.0f, 1.0f};
+  nbx_draw d;
+  nbx_draw_default(&d);
+  RenderParams P{};
+  render_params(&cam, &d, 1, 1, P);
+  unsigned long long entries = 0;
+  int rc = render_prepare(h, P, &entries);
+  if (rc != NBX_OK) return rc;
+  NBX_CUDA(h, cudaMemcpy(stats, h->rs.stats, 3 * sizeof(float), cudaMemcpyDeviceToHost));
+  return NBX_OK;
+}
+
+int nbx_render(nbx_handle *h, const nbx_camera *cam, const nbx_draw *d, uint32_t width,
+               uint32_t height, float *rgba, float *stats) {
+  if (!h) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  RenderParams P{};
+  if (render_params(cam, d, width, height, P) != NBX_OK)
+    return fail(h, NBX_ERR_ARG, "bad camera, draw settings or image size");
+  if (!h->uploaded) return fail(h, NBX_ERR_STATE, "no bodies uploaded");
+  auto &r = h->rs;
+  const size_t pixels = (size_t)width * height;
+  const uint32_t tiles = P.tilesX * P.tilesY;
+  if (r.pixels < pixels || !r.image) {
+    NBX_CUDA(h, grow(r.image, pixels));
+    r.pixels = pixels;
+  }
+  if (r.tiles < tiles || !r.first) {
+    NBX_CUDA(h, grow(r.first, tiles));
+    NBX_CUDA(h, grow(r.last, tiles));
+    r.tiles = tiles;
+  }
+  unsigned long long entries = 0;
+  if (h->n > 0) {
+    int rc = render_prepare(h, P, &entries);
+    if (rc != NBX_OK) return rc;
+  }
+  if (entries > (1ull << 30))
+    return fail(h, NBX_ERR_CAPACITY,
+                "splats cover more than 2^30 (tile, body) pairs: zoom out or shrink the image");
+  const uint32_t m = (uint32_t)entries;
+  if (m > r.entries || !r.sort.keys[0]) {
+    SortScratch &so = r.sort;
+    const uint32_t cap = std::max<uint32_t>(m, 1024);
+    NBX_CUDA(h, grow(so.keys[0], cap));
+    NBX_CUDA(h, grow(so.keys[1], cap));
+    NBX_CUDA(h, grow(so.vals[0], cap));
+    NBX_CUDA(h, grow(so.vals[1], cap));
+    if (!so.hist) NBX_CUDA(h, cudaMalloc(&so.hist, 8 * 256 * sizeof(uint32_t)));
+    if (!so.tileCounter) NBX_CUDA(h, cudaMalloc(&so.tileCounter, 8 * sizeof(uint32_t)));
+    so.capacity = cap;
+    so.maxTiles = (uint32_t)sort_tiles(cap);
+    NBX_CUDA(h, grow(so.status, (size_t)so.maxTiles * 256 + 256));
+    r.entries = cap;
+  }
+  int bits = 8;
+  while (bits < 32 && (1ull << bits) < tiles) bits += 8;
+  cudaStream_t s = h->stream;
+  int buf = 0;
+  if (m > 0) {
+    exclusive_scan_u32(s, r.count, r.off, h->n, nullptr, nullptr, h->scan, h->base.status);
+    render_emit(s, r.v0, r.off, h->n, P, r.sort.keys[0], r.sort.vals[0]);
+    NBX_CUDA(h, cudaMemcpyAsync(r.total + 1, &m, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    buf = radix_sort_u64(s, r.sort, m, reinterpret_cast<const uint32_t *>(r.total + 1), 0,
+                         bits, false, false, h->base.status);
+  }
+  render_composite(s, r.v0, r.v1, r.sort.keys[buf], r.sort.vals[buf],
+                   reinterpret_cast<const uint32_t *>(r.total + 1), m, r.first, r.last, P,
+                   r.image);
+  NBX_CUDA(h, cudaGetLastError());
+  if (rgba)
+    NBX_CUDA(h, cudaMemcpyAsync(rgba, r.image, pixels * sizeof(float4), cudaMemcpyDeviceToHost, s));
+  float st[3] = {0.0f, 0.0f, 1.0f};
+  if (h->n > 0)
+    NBX_CUDA(h, cudaMemcpyAsync(st, r.stats, sizeof(st), cudaMemcpyDeviceToHost, s));
+  NBX_CUDA(h, cudaStreamSynchronize(s));
+  if (stats) std::memcpy(stats, st, sizeof(st));
+  return check_status(h);
+}
+
 int nbx_set_attractor(nbx_handle *h, int active, float x, float y, float mass,
                       float softening) {
   if (!h) return NBX_ERR_ARG;
@@ -951,6 +1137,7 @@ int nbx_reset(nbx_handle *h, const nbx_body *bodies, size_t n) {
   // pending frames are written first; the writer is rebuilt for the new size
   const int frc = frames_flush(h);
   frames_destroy(h);
+  render_free(h);
   if (frc != NBX_OK) return fail(h, frc, "writing a recorded NBS2 frame failed");
   // keep the network parameters across the reallocation (optimizer
   // moments start again)

@@ -114,6 +114,14 @@ struct DevState {
   float4 *attr;
 };
 
+// Camera and draw settings of the splat renderer (render.cu).
+struct RenderParams {
+  float camX, camY, scale, halfW, halfH;
+  uint32_t width, height, tilesX, tilesY;
+  int mode; // 0 speed ramp, over-composited; 1 glow, additive
+  float pointScale, minPoint, brightness, speedMax;
+};
+
 // The viewer's attractor pull (attractorKernel, src/cuda/CudaSimulation.cu
 // :14-31): acc += d * m / (sqrt(|d|^2 + 1e-12) (|d|^2 + soft^2)), d = a - p,
 // added after the gravitational sum.  kExact: IEEE reciprocal square root

@@ -40,6 +40,7 @@ EXPORTS = (
     "nbx_make_scenario", "nbx_renumber", "nbx_add_heavy_body", "nbx_add_cluster",
     "nbx_set_attractor", "nbx_reset", "nbx_nbs2_record", "nbx_nbs2_flush",
     "nbx_nbs2_open", "nbx_nbs2_write_packed", "nbx_nbs2_close",
+    "nbx_draw_default", "nbx_render", "nbx_body_stats",
 )
 SCENARIOS = {"disc": 0, "two_galaxies": 1, "cold_square": 2}
 MLP_PARAMS = 1442
@@ -59,6 +60,19 @@ class Params(C.Structure):
                 ("node_factor", C.c_float), ("pair_factor", C.c_float),
                 ("force_blocks", C.c_int32), ("device", C.c_int32),
                 ("mlp_band", C.c_float), ("force_law", C.c_int32)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("center_x", C.c_float), ("center_y", C.c_float), ("scale", C.c_float)]
+
+
+class Draw(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("point_scale", C.c_float),
+                ("min_point_px", C.c_float), ("brightness", C.c_float),
+                ("speed_max", C.c_float)]
+
+
+DRAW_MODES = {"speed": 0, "glow": 1}
 
 
 class NbxError(RuntimeError):
@@ -98,6 +112,10 @@ def lib() -> C.CDLL:
         "nbx_force_times": [vp, vp, C.c_uint32],
         "nbx_make_scenario": [C.c_int, C.c_uint32, C.c_uint32, vp],
         "nbx_set_attractor": [vp, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float],
+        "nbx_draw_default": [C.POINTER(Draw)],
+        "nbx_render": [vp, C.POINTER(Camera), C.POINTER(Draw), C.c_uint32, C.c_uint32,
+                       vp, vp],
+        "nbx_body_stats": [vp, vp],
         "nbx_reset": [vp, vp, C.c_size_t],
         "nbx_sync": [vp],
         "nbx_phase": [vp, C.c_int],
@@ -205,6 +223,15 @@ class Nbs2Writer:
         if self.f:
             _check(None, lib().nbx_nbs2_close(self.f))
             self.f = None
+
+
+def save_ppm(rgba: np.ndarray, path) -> None:
+    """Writes a rendered image as an 8-bit binary PPM (top row first)."""
+    rgb = np.clip(rgba[::-1, :, :3], 0.0, 1.0)
+    data = (rgb * 255.0 + 0.5).astype(np.uint8)
+    with open(path, "wb") as f:
+        f.write(b"P6\n%d %d\n255\n" % (data.shape[1], data.shape[0]))
+        f.write(data.tobytes())
 
 
 def make_scenario(kind: str, n: int, seed: int = 0) -> np.ndarray:
@@ -317,6 +344,25 @@ class Handle:
 
     def step(self, steps: int = 1):
         self._c(lib().nbx_step(self.h, steps))
+
+    def render(self, width: int, height: int, center=(0.0, 0.0), scale=1.0,
+               mode="glow", point_scale=1.0, min_point=1.5, brightness=0.6,
+               speed_max=60.0):
+        """The viewer's splat drawing on the GPU: (rgba[height, width, 4]
+        premultiplied, row 0 at the bottom; {com_x, com_y, max_speed})."""
+        cam = Camera(center[0], center[1], scale)
+        d = Draw(DRAW_MODES[mode] if isinstance(mode, str) else int(mode), point_scale,
+                 min_point, brightness, speed_max)
+        img = np.zeros((height, width, 4), np.float32)
+        st = np.zeros(3, np.float32)
+        self._c(lib().nbx_render(self.h, C.byref(cam), C.byref(d), width, height,
+                                 img.ctypes.data, st.ctypes.data))
+        return img, {"com_x": float(st[0]), "com_y": float(st[1]), "max_speed": float(st[2])}
+
+    def body_stats(self) -> dict:
+        st = np.zeros(3, np.float32)
+        self._c(lib().nbx_body_stats(self.h, st.ctypes.data))
+        return {"com_x": float(st[0]), "com_y": float(st[1]), "max_speed": float(st[2])}
 
     def nbs2_record(self, writer: "Nbs2Writer"):
         """Records the current state as writer's next frame (device path)."""

@@ -927,3 +927,84 @@ void orc_attractor(size_t n, const float *x, const float *y, float axp, float ay
     ay[i] = ay[i] + dy * f;
   }
 }
+
+static float orc_mixf(float x, float y, float a) { return x * (1.0f - a) + y * a; }
+
+static void orc_ramp(float t, float c[3]) {
+  static const float slow[3] = {0.15f, 0.3f, 1.0f}, mid[3] = {0.2f, 0.95f, 1.0f},
+                     fast[3] = {1.0f, 0.9f, 0.55f};
+  t = fminf(fmaxf(t, 0.0f), 1.0f);
+  if (t < 0.5f) {
+    const float u = t * 2.0f;
+    for (int k = 0; k < 3; ++k) c[k] = orc_mixf(slow[k], mid[k], u);
+  } else {
+    const float u = t * 2.0f - 1.0f;
+    for (int k = 0; k < 3; ++k) c[k] = orc_mixf(mid[k], fast[k], u);
+  }
+}
+
+static int orc_pixel_range(float wpos, float hf, uint32_t extent, int *lo, int *hi) {
+  const float a = wpos - hf, b = wpos + hf;
+  if (!(a < (float)extent) || !(b >= 0.0f)) return 0;
+  *lo = a <= 0.0f ? 0 : (int)floorf(a);
+  *hi = b >= (float)(extent - 1) ? (int)extent - 1 : (int)floorf(b);
+  return *lo <= *hi;
+}
+
+void orc_render(size_t n, const orc_body *b, float camX, float camY, float scale,
+                int mode, float pointScale, float minPoint, float brightness,
+                float speedMax, uint32_t w, uint32_t h, float *rgba, float *stats) {
+  for (size_t p = 0; p < (size_t)w * h; ++p) {
+    rgba[4 * p + 0] = 0.0f;
+    rgba[4 * p + 1] = 0.0f;
+    rgba[4 * p + 2] = 0.02f;
+    rgba[4 * p + 3] = 1.0f;
+  }
+  const float halfW = (float)w * 0.5f, halfH = (float)h * 0.5f;
+  double mx = 0.0, my = 0.0, m = 0.0;
+  float vmax = 0.0f;
+  for (size_t i = 0; i < n; ++i) {
+    const float speed = sqrtf(b[i].vx * b[i].vx + b[i].vy * b[i].vy);
+    m += b[i].mass;
+    mx += (double)b[i].mass * b[i].px;
+    my += (double)b[i].mass * b[i].py;
+    vmax = fmaxf(vmax, speed);
+    const float wx = (b[i].px - camX) * scale + halfW;
+    const float wy = (b[i].py - camY) * scale + halfH;
+    const float size = b[i].radius * 2.0f * scale * pointScale;
+    const float ps = fmaxf(size, minPoint);
+    const float alpha = fminf(fmaxf(size / minPoint, 0.08f), 1.0f);
+    const float hf = ps * 0.5f;
+    float c[3] = {0.35f, 0.75f, 1.0f};
+    if (mode == 0) orc_ramp(speed / speedMax, c);
+    int x0, x1, y0, y1;
+    if (!orc_pixel_range(wx, hf, w, &x0, &x1) || !orc_pixel_range(wy, hf, h, &y0, &y1))
+      continue;
+    for (int py = y0; py <= y1; ++py) {
+      for (int px = x0; px <= x1; ++px) {
+        const float cx = (float)px + 0.5f, cy = (float)py + 0.5f;
+        const float dx = (cx - wx) / hf, dy = (cy - wy) / hf;
+        const float r2 = dx * dx + dy * dy;
+        if (r2 > 1.0f) continue;
+        const float a = (1.0f - r2) * alpha * brightness;
+        float *d = rgba + 4 * ((size_t)py * w + px);
+        const float s0 = c[0] * a, s1 = c[1] * a, s2 = c[2] * a;
+        if (mode == 1) {
+          d[0] = s0 + d[0];
+          d[1] = s1 + d[1];
+          d[2] = s2 + d[2];
+          d[3] = a + d[3];
+        } else {
+          const float k1 = 1.0f - a;
+          d[0] = s0 + d[0] * k1;
+          d[1] = s1 + d[1] * k1;
+          d[2] = s2 + d[2] * k1;
+          d[3] = a + d[3] * k1;
+        }
+      }
+    }
+  }
+  stats[0] = m > 0.0 ? (float)(mx / m) : 0.0f;
+  stats[1] = m > 0.0 ? (float)(my / m) : 0.0f;
+  stats[2] = vmax > 0.0f ? vmax : 1.0f;
+}

@@ -119,6 +119,16 @@ int orc_naive_step(size_t n, orc_body *b, float dt, float epsilon, int collision
 void orc_attractor(size_t n, const float *x, const float *y, float axp, float ayp,
                    float mass, float softening, float *ax, float *ay);
 
+/* The viewer's point-sprite drawing restated (src/viewer/Renderer.cpp:8-52
+ * shaders, 113-147 blending; the product's headless renderer defines the
+ * same math): bodies in array order into rgba[h][w][4], row 0 at the
+ * bottom, cleared to (0, 0, 0.02, 1); mode 0 speed ramp composited over,
+ * mode 1 glow additive.  stats = {comX, comY, maxSpeed} as BodyStats
+ * (Interop.cu:80-104), sums in FP64 in index order. */
+void orc_render(size_t n, const orc_body *b, float camX, float camY, float scale,
+                int mode, float pointScale, float minPoint, float brightness,
+                float speedMax, uint32_t w, uint32_t h, float *rgba, float *stats);
+
 /* FP64 direct sum with the tree's force law for the given targets
  * (exactTreeLawForces, src/cuda/CheckCuda.cu:453-475; eps generalised). */
 void orc_direct_fp64(size_t n, const float *x, const float *y, const float *m,

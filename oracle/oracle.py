@@ -113,6 +113,8 @@ class Oracle:
         L.orc_naive_step.restype = C.c_int
         L.orc_attractor.argtypes = [C.c_size_t, _f32p, _f32p, C.c_float, C.c_float,
                                     C.c_float, C.c_float, _f32p, _f32p]
+        L.orc_render.argtypes = [C.c_size_t, _bodyp] + [C.c_float] * 3 + [C.c_int] + \
+                                [C.c_float] * 4 + [C.c_uint32, C.c_uint32, _f32p, _f32p]
         L.orc_direct_fp64.argtypes = [C.c_size_t, _f32p, _f32p, _f32p,
                                       C.c_double, C.c_size_t, _u32p, _f64p,
                                       _f64p]
@@ -254,6 +256,16 @@ class Oracle:
                              np.ascontiguousarray(y, np.float32), at[0], at[1],
                              mass, softening, ax, ay)
         return ax, ay
+
+    def render(self, b, width, height, center=(0.0, 0.0), scale=1.0, mode=1,
+               point_scale=1.0, min_point=1.5, brightness=0.6, speed_max=60.0):
+        """The viewer's splat drawing restated; returns (rgba[h, w, 4], stats)."""
+        img = np.zeros((height, width, 4), np.float32)
+        st = np.zeros(3, np.float32)
+        self.L.orc_render(len(b), np.ascontiguousarray(b), center[0], center[1], scale,
+                          mode, point_scale, min_point, brightness, speed_max, width,
+                          height, img.reshape(-1), st)
+        return img, st
 
     def direct_fp64(self, b: np.ndarray, eps, targets):
         targets = np.ascontiguousarray(targets, np.uint32)
