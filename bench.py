@@ -248,6 +248,25 @@ def forms_leg(nbx, torch, sim, n, local, ids, args):
     return out
 
 
+def render_leg(nbx, sim, n):
+    """The headless splat renderer on the headline state: 1920x1080, both
+    colour modes, camera fitted to the bodies; wall time per frame (each
+    call synchronises)."""
+    st = sim.body_stats()
+    res = {"width": 1920, "height": 1080, "bodies": n}
+    s = sim.download()
+    span = max(float(np.ptp(s["px"])), float(np.ptp(s["py"])), 1.0) * 1.1
+    for mode in ("glow", "speed"):
+        for _ in range(3):
+            sim.render(1920, 1080, (st["com_x"], st["com_y"]), 1080 / span, mode=mode)
+        t0 = time.perf_counter()
+        reps = 10
+        for _ in range(reps):
+            sim.render(1920, 1080, (st["com_x"], st["com_y"]), 1080 / span, mode=mode)
+        res[f"{mode}_ms_per_frame"] = (time.perf_counter() - t0) * 1e3 / reps
+    return res
+
+
 NAIVE_N = 1 << 18
 
 
@@ -462,6 +481,7 @@ def run_b200(args):
     sim_keep = sim
     ens = ensemble_leg(nbx, torch, world, rank, local, dist, args) if not args.quick else None
     naive = naive_leg(nbx, torch, local, args) if not args.quick else None
+    render = render_leg(nbx, sim_keep, n) if not args.quick else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -525,6 +545,8 @@ def run_b200(args):
         line["ensemble"] = ens
     if naive is not None:
         line["naive"] = naive
+    if render is not None:
+        line["render"] = render
     if cpu is not None:
         line["cpu_baseline"] = cpu
     if rank == 0:
