@@ -8,8 +8,9 @@
 // kStatusSpinLimit in the caller's status word and carries on with what it
 // has, so a stuck predecessor can never hang the GPU.
 //
-// The radix sort is stable (ranks within a warp come from __match_any_sync
-// over warp-striped items, in input order), so equal keys keep their input
+// The radix sort is stable (ranks within a warp come from the lanes sharing
+// a digit, found with one ballot per digit bit, over warp-striped items in
+// input order), so equal keys keep their input
 // order exactly as cub::DeviceRadixSort::SortPairs does
 // (CudaQuadTree.cu:405-407), which the Morton permutation parity needs.
 #include "nbx_internal.cuh"
@@ -229,10 +230,24 @@ __global__ void __launch_bounds__(kSortThreads)
     dig[k] = ok ? (uint32_t)((key[k] >> shift) & 255u) : 256u;
   }
   const uint32_t ltmask = lanemask_lt();
+  // lanes holding the same digit, from one ballot per digit bit (plus one
+  // for validity); all items' masks first, so the ballots overlap
+  uint32_t peer[kSortItems];
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
     const uint32_t d = dig[k];
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    uint32_t m = __ballot_sync(0xffffffffu, d < 256u);
+#pragma unroll
+    for (int bit = 0; bit < 8; ++bit) {
+      const uint32_t bb = __ballot_sync(0xffffffffu, (d >> bit) & 1u);
+      m &= ((d >> bit) & 1u) ? bb : ~bb;
+    }
+    peer[k] = m;
+  }
+#pragma unroll
+  for (int k = 0; k < kSortItems; ++k) {
+    const uint32_t d = dig[k];
+    const uint32_t peers = peer[k];
     const uint32_t before = __popc(peers & ltmask);
     uint32_t b = 0;
     if (d < 256u) b = s_whist[warp][d];
