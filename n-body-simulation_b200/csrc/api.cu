@@ -347,6 +347,7 @@ int allocate(nbx_handle *h) {
   A(S.chain, S.pairCapacity);
   A(S.unitOrder, n);
   A(S.counters, 16);
+  A(S.longRuns, n / 16 + 64);
   A(S.codes, n);
   A(S.perm, n);
   A(S.sortedCodes, n);

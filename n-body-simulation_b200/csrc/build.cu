@@ -71,7 +71,9 @@ __global__ void k_root_frame(DevState S) {
   b[3] = 0u;
 }
 
-// Morton code of every body; digit histograms of the 8 sort passes fused.
+// Morton code of every body; digit histograms of the radix passes fused
+// (the passes over the high 32 bits: kMortonSortPass0 .. 7).
+constexpr int kMortonSortPass0 = 4;
 __global__ void __launch_bounds__(kBlock)
     k_morton(DevState S, uint64_t *__restrict__ keys, uint32_t *hist) {
   __shared__ uint32_t sh[8][256];
@@ -86,10 +88,10 @@ __global__ void __launch_bounds__(kBlock)
     keys[i] = c;
     S.codes[i] = c;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) atomicAdd(&sh[q][(c >> (8 * q)) & 255u], 1u);
+    for (int q = kMortonSortPass0; q < 8; ++q) atomicAdd(&sh[q][(c >> (8 * q)) & 255u], 1u);
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) {
+  for (int i = kMortonSortPass0 * 256 + threadIdx.x; i < 8 * 256; i += blockDim.x) {
     const uint32_t v = sh[i >> 8][i & 255];
     if (v) atomicAdd(&hist[i], v);
   }
@@ -514,7 +516,14 @@ void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
   cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * 8 * 256, s);
   k_morton<<<grid_for(n), kBlock, 0, s>>>(S, sort.keys[0], sort.hist);
   mark(s, "build.morton");
-  int buf = radix_sort_u64(s, sort, n, nullptr, 0, 64, true, true, S.status);
+  // radix passes over the high 32 bits (depth-16 cells), then every run of
+  // equal high bits is ordered by its low bits: the same stable order as a
+  // full 64-bit sort; such runs are rare and short (at most 2 bodies in the
+  // headline states), so this replaces four full passes
+  int buf = radix_sort_u64(s, sort, n, nullptr, 8 * kMortonSortPass0, 64, true, true,
+                           S.status);
+  sort_fix_low_bits(s, sort, buf, n, 8 * kMortonSortPass0, S.longRuns, &S.counters[9],
+                    n / 16 + 64, S.status);
   mark(s, "build.sort");
   if (S.nseg > 1) {
     // stable passes on the instance id keep instances in their ranges

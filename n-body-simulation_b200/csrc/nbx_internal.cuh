@@ -126,6 +126,8 @@ struct SortScratch {
 };
 
 size_t sort_tiles(uint32_t n_max);
+void sort_fix_low_bits(cudaStream_t s, SortScratch &sc, int buf, uint32_t n, int shift,
+                       uint32_t *longRuns, uint32_t *runCount, uint32_t cap, uint32_t *err);
 
 // Stable LSD radix sort of (keys[0], vals[0]) on key bits [bit_lo, bit_hi)
 // (multiples of 8).  If `have_hist` the caller already filled

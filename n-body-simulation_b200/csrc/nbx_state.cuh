@@ -79,9 +79,11 @@ struct DevState {
   uint32_t *unitFlag;    // nLater > 0
   uint32_t *unitPos;     // scan of unitFlag
   uint32_t *unitOrder;   // units in before() order (last collide)
+  uint32_t *longRuns;    // Morton sort: starts of runs of > 16 equal high keys
   uint32_t *counters;    // [0]=pairs*2 total [1]=units [2]=unit claim
                          // [3]=splitting entries [4]=total nodes
                          // [5]=small-large pairs [8]=id check
+                         // [9]=long Morton runs
 
   // Morton / sort
   uint64_t *codes; // unsorted codes (kept for the segment passes)

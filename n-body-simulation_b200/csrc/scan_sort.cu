@@ -353,7 +353,170 @@ __global__ void __launch_bounds__(kSortThreads)
   }
 }
 
+constexpr uint32_t kShortRun = 16; // runs up to this length: one thread
+
+// Keys sorted (stably) by their bits >= shift only: every run of equal high
+// bits is put in order of its low bits, stably, in place.  Runs of up to
+// kShortRun keys are insertion-sorted by the thread at their start; longer
+// ones are listed for k_long_runs.  Reordering inside a run never changes
+// the high bits the other threads compare, so run detection is unaffected.
+__global__ void __launch_bounds__(256)
+    k_fix_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t n,
+               int shift, uint32_t *__restrict__ longRuns, uint32_t *longCount,
+               uint32_t cap, uint32_t *err) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    const uint64_t hi = keys[i] >> shift;
+    if (i > 0 && (keys[i - 1] >> shift) == hi) continue; // not a run start
+    if (i + 1 >= n || (keys[i + 1] >> shift) != hi) continue; // single key
+    uint32_t len = 2;
+    while (i + len < n && len <= kShortRun && (keys[i + len] >> shift) == hi) ++len;
+    if (len > kShortRun) {
+      const uint32_t slot = atomicAdd(longCount, 1u);
+      if (slot < cap) longRuns[slot] = i;
+      else atomicOr(err, kStatusSpinLimit);
+      continue;
+    }
+    uint64_t k[kShortRun];
+    uint32_t v[kShortRun];
+    for (uint32_t a = 0; a < len; ++a) {
+      k[a] = keys[i + a];
+      v[a] = vals[i + a];
+    }
+    for (uint32_t a = 1; a < len; ++a) { // stable: equal keys keep their order
+      const uint64_t kk = k[a];
+      const uint32_t vv = v[a];
+      uint32_t b = a;
+      while (b > 0 && k[b - 1] > kk) {
+        k[b] = k[b - 1];
+        v[b] = v[b - 1];
+        --b;
+      }
+      k[b] = kk;
+      v[b] = vv;
+    }
+    for (uint32_t a = 0; a < len; ++a) {
+      keys[i + a] = k[a];
+      vals[i + a] = v[a];
+    }
+  }
+}
+
+// One block per long run: a stable LSD radix sort of the run on its bits
+// below `shift` (shift / 8 passes through tmp, which holds the same index
+// range), tile by tile in input order so equal digits keep their order.
+__global__ void __launch_bounds__(256)
+    k_long_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                uint64_t *__restrict__ tmpK, uint32_t *__restrict__ tmpV, uint32_t n,
+                int shift, const uint32_t *__restrict__ longRuns, const uint32_t *longCount,
+                uint32_t cap) {
+  __shared__ uint32_t sHist[256], sOff[256], sWarp[8][256];
+  __shared__ uint32_t sEnd;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t runs = min(*longCount, cap);
+  const uint32_t ltmask = lanemask_lt();
+  for (uint32_t r = blockIdx.x; r < runs; r += gridDim.x) {
+    const uint32_t s0 = longRuns[r];
+    const uint64_t hi = keys[s0] >> shift;
+    // run end: the first key past s0 with other high bits
+    if (tid == 0) sEnd = n;
+    __syncthreads();
+    for (uint32_t base = s0; base < n; base += 256) {
+      const uint32_t i = base + tid;
+      if (i < n && (keys[i] >> shift) != hi) atomicMin(&sEnd, i);
+      __syncthreads();
+      const bool found = sEnd != n;
+      __syncthreads(); // every thread has read sEnd before the next tile
+      if (found) break;
+    }
+    const uint32_t e0 = sEnd;
+    uint64_t *srcK = keys, *dstK = tmpK;
+    uint32_t *srcV = vals, *dstV = tmpV;
+    for (int p = 0; p * 8 < shift; ++p) {
+      const int sh = 8 * p;
+      sHist[tid] = 0;
+      __syncthreads();
+      for (uint32_t i = s0 + tid; i < e0; i += 256)
+        atomicAdd(&sHist[(uint32_t)(srcK[i] >> sh) & 255u], 1u);
+      __syncthreads();
+      if (tid == 0) {
+        uint32_t run = s0;
+        for (int d = 0; d < 256; ++d) {
+          sOff[d] = run;
+          run += sHist[d];
+        }
+      }
+      __syncthreads();
+      for (uint32_t base = s0; base < e0; base += 256) {
+        const uint32_t i = base + tid;
+        const bool ok = i < e0;
+        const uint64_t k = ok ? srcK[i] : 0ull;
+        const uint32_t v = ok ? srcV[i] : 0u;
+        const uint32_t d = ok ? ((uint32_t)(k >> sh) & 255u) : 256u;
+        uint32_t peers = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+        for (int bit = 0; bit < 8; ++bit) {
+          const uint32_t bb = __ballot_sync(0xffffffffu, (d >> bit) & 1u);
+          peers &= ((d >> bit) & 1u) ? bb : ~bb;
+        }
+        for (int w = 0; w < 8; ++w) sWarp[w][tid] = 0;
+        __syncthreads();
+        if (ok && __popc(peers & ltmask) == 0) sWarp[warp][d] = __popc(peers);
+        __syncthreads();
+        // exclusive prefix over warps per digit, tile total into the offsets
+        {
+          uint32_t acc = 0;
+          for (int w = 0; w < 8; ++w) {
+            const uint32_t c = sWarp[w][tid];
+            sWarp[w][tid] = acc;
+            acc += c;
+          }
+          sHist[tid] = acc; // this tile's count of digit tid
+        }
+        __syncthreads();
+        if (ok) {
+          const uint32_t dst = sOff[d] + sWarp[warp][d] + __popc(peers & ltmask);
+          dstK[dst] = k;
+          dstV[dst] = v;
+        }
+        __syncthreads();
+        sOff[tid] += sHist[tid];
+        __syncthreads();
+      }
+      uint64_t *tk = srcK;
+      srcK = dstK;
+      dstK = tk;
+      uint32_t *tv = srcV;
+      srcV = dstV;
+      dstV = tv;
+    }
+    if (srcK != keys) { // odd number of passes: copy back
+      for (uint32_t i = s0 + tid; i < e0; i += 256) {
+        keys[i] = srcK[i];
+        vals[i] = srcV[i];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 } // namespace
+
+// Completes a sort that ran its radix passes on the bits >= shift only:
+// orders every run of equal high bits by the low bits (stable), in place in
+// sc.keys[buf] / sc.vals[buf].  longRuns holds cap run starts; *runCount is
+// device scratch.
+void sort_fix_low_bits(cudaStream_t s, SortScratch &sc, int buf, uint32_t n, int shift,
+                       uint32_t *longRuns, uint32_t *runCount, uint32_t cap, uint32_t *err) {
+  if (n < 2) return;
+  cudaMemsetAsync(runCount, 0, sizeof(uint32_t), s);
+  uint32_t b = (n + 255) / 256;
+  if (b > 148u * 16u) b = 148u * 16u;
+  k_fix_runs<<<b, 256, 0, s>>>(sc.keys[buf], sc.vals[buf], n, shift, longRuns, runCount,
+                               cap, err);
+  k_long_runs<<<148, 256, 0, s>>>(sc.keys[buf], sc.vals[buf], sc.keys[buf ^ 1],
+                                   sc.vals[buf ^ 1], n, shift, longRuns, runCount, cap);
+}
 
 size_t sort_tiles(uint32_t n_max) {
   return (n_max + kSortTile - 1) / kSortTile + 1;

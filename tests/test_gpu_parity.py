@@ -59,6 +59,17 @@ def state(nbx, oracle, name):
         sim.phase("iterate")
         s = sim.download()
         sim.close()
+    elif name == "clumped":
+        # tight clumps inside depth-16 Morton cells: runs of equal high code
+        # bits of 17 to ~3000 bodies with distinct low bits
+        s = nbx.uniform_disc(20000)
+        rng = np.random.default_rng(3)
+        for start, count, cx, cy, size in ((100, 17, 3.0, -2.0, 1e-3),
+                                           (2000, 500, 10.0, 5.0, 1e-2),
+                                           (5000, 3000, -20.0, 30.0, 1.5e-2)):
+            sl = slice(start, start + count)
+            s["px"][sl] = (cx + rng.uniform(-size, size, count)).astype(np.float32)
+            s["py"][sl] = (cy + rng.uniform(-size, size, count)).astype(np.float32)
     elif name == "coincident":
         s = nbx.uniform_disc(3000)
         s["px"][100:160] = s["px"][100]  # 60 bodies on one point: depth-32 leaf
@@ -70,7 +81,7 @@ def state(nbx, oracle, name):
 
 
 @pytest.mark.parametrize("name", ["disc10k", "disc200k", "two_discs65k",
-                                  "cold50k", "coincident"])
+                                  "cold50k", "coincident", "clumped"])
 @pytest.mark.parametrize("leaf", [16, 4])
 def test_morton_perm_tree_bit_exact(nbx, oracle, name, leaf):
     b = state(nbx, oracle, name)
@@ -89,7 +100,8 @@ def test_morton_perm_tree_bit_exact(nbx, oracle, name, leaf):
     sim.close()
 
 
-@pytest.mark.parametrize("name", ["disc10k", "disc200k", "colliding20k", "cold50k"])
+@pytest.mark.parametrize("name", ["disc10k", "disc200k", "colliding20k", "cold50k",
+                                  "clumped"])
 @pytest.mark.parametrize("theta", [1.0, 0.5])
 def test_forces(nbx, oracle, name, theta):
     b = state(nbx, oracle, name)
