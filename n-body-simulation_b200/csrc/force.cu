@@ -98,7 +98,9 @@ __device__ __forceinline__ void quad_term(float dx, float dy, float dSq,
                                           float iyy, float ixy, float &qx,
                                           float &qy) {
   const float q = dSq + eSq;
-  const float iq = 1.0f / q, ir2 = 1.0f / dSq;
+  // a correction term: the hardware reciprocal's ~1 ulp is far below its
+  // own truncation error
+  const float iq = rcp_approx(q), ir2 = rcp_approx(dSq);
   const float c3 = 3.0f * dSq + eSq;
   const float aOverG = -c3 * ir2 * iq;                        // g'/(r g)
   const float gpp = -6.0f * iq + c3 * (2.0f * ir2 * iq + 4.0f * iq * iq);
@@ -106,7 +108,7 @@ __device__ __forceinline__ void quad_term(float dx, float dy, float dSq,
   const float Idx = ixx * dx + ixy * dy, Idy = ixy * dx + iyy * dy;
   const float tr = ixx + iyy;
   const float dId = dx * Idx + dy * Idy;
-  const float h = 0.5f / mass;
+  const float h = 0.5f * rcp_approx(mass);
   qx = h * (aOverG * (2.0f * Idx + tr * dx) + bOverG * dx * dId);
   qy = h * (aOverG * (2.0f * Idy + tr * dy) + bOverG * dy * dId);
 }
