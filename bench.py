@@ -271,6 +271,33 @@ def render_leg(nbx, sim, n):
     return res
 
 
+def cold_square_leg(nbx, torch, local):
+    """The collision-heavy cold-square collapse at its full size: 4,194,304
+    unit masses at rest (the viewer's ColdSquare geometry, softening 1e-3 of
+    the half-width), theta 0.5, collisions on; 200 steps (the configuration
+    runs 2000); momentum and angular momentum from compensated FP64 sums."""
+    n = 1 << 22
+    eps = 1e-3 * 3.0 * float(np.sqrt(n))
+    sim = nbx.Simulation(nbx.cold_square(n, 0), theta=0.5, epsilon=eps, device=local)
+    stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+    em0 = sim.energy_momentum()
+    sim.step(3)
+    sim.sync()
+    steps = 200
+    ms = time_steps(torch, sim, stream, steps)
+    em = sim.energy_momentum()
+    s = sim.download()
+    mv = float(np.sum(s["mass"].astype(np.float64)
+                      * np.hypot(s["vx"].astype(np.float64), s["vy"].astype(np.float64))))
+    sim.close()
+    return {"bodies": n, "steps": steps, "epsilon": eps, "ms_per_step": ms,
+            "body_steps_per_s": n / (ms * 1e-3),
+            "kinetic_energy_fp64": float(em[0]),
+            "momentum_drift_rel": float(np.hypot(em[1] - em0[1], em[2] - em0[2])) / mv,
+            "angular_momentum_drift_rel": float(abs(em[3] - em0[3])) / (mv * 3.0 * np.sqrt(n)),
+            "mass_exact": bool(em[4] == em0[4])}
+
+
 NAIVE_N = 1 << 18
 
 
@@ -485,6 +512,7 @@ def run_b200(args):
     sim_keep = sim
     ens = ensemble_leg(nbx, torch, world, rank, local, dist, args) if not args.quick else None
     naive = naive_leg(nbx, torch, local, args) if not args.quick else None
+    cold = cold_square_leg(nbx, torch, local) if not args.quick else None
     render = render_leg(nbx, sim_keep, n) if not args.quick else None
 
     cpu = None
@@ -549,6 +577,8 @@ def run_b200(args):
         line["ensemble"] = ens
     if naive is not None:
         line["naive"] = naive
+    if cold is not None:
+        line["cold_square"] = cold
     if render is not None:
         line["render"] = render
     if cpu is not None:
