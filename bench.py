@@ -184,7 +184,7 @@ def run_reference(args):
     if rank != 0:
         return
     steps = max(1, min(args.steps, 20))
-    warm = max(1, min(args.warmup, 2))
+    warm = max(3, min(args.warmup, 5))
     value, cores, ms = reference_rate(args.n, steps, warm)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
