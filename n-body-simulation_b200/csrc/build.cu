@@ -426,10 +426,14 @@ __global__ void __launch_bounds__(kBlock) k_upward(DevState S) {
         break;
       }
       const uint32_t pg = nb + (uint32_t)node;
-      __threadfence();
-      const uint32_t old = atomicAdd(&S.arrive[pg], 1u);
+      // release: this child's sums are visible to the last arriver; acquire:
+      // the last arriver sees all four children's sums
+      uint32_t old;
+      asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;"
+                   : "=r"(old)
+                   : "l"(&S.arrive[pg])
+                   : "memory");
       if (old != 3u) break;
-      __threadfence();
       const uint32_t c = nb + (uint32_t)S.children[pg];
       float sx = __ldcg(&S.sumX[c]), sy = __ldcg(&S.sumY[c]),
             sm = __ldcg(&S.mass[c]);
