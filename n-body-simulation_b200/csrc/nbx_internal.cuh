@@ -94,7 +94,7 @@ __device__ __forceinline__ uint32_t load_count(const uint32_t *d_n, uint32_t n) 
 // Device-wide primitives (scan_sort.cu).  All take a stream and never
 // synchronise with the host, so they can be captured in a CUDA graph.
 struct ScanScratch {
-  uint64_t *status = nullptr; // one word per tile
+  uint64_t *status = nullptr; // per tile: its sum (low 32 bits used)
   uint32_t *tileCounter = nullptr;
   uint32_t maxTiles = 0;
 };

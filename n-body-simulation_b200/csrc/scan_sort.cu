@@ -1,8 +1,10 @@
-// scan_sort.cu -- single-pass exclusive scan and onesweep LSD radix sort.
+// scan_sort.cu -- exclusive scan and onesweep LSD radix sort.
 //
-// Both use decoupled look-back (Merrill & Garland 2016; Adinets & Merrill
-// 2022, "Onesweep"): tiles are claimed in order through an atomic
-// counter, each tile publishes its aggregate, and looks back over its
+// The scan reduces every tile first and then lets each tile add the sums
+// of the tiles before it: two launches with no dependence between tiles.
+// The radix sort uses decoupled look-back (Merrill & Garland 2016; Adinets &
+// Merrill 2022, "Onesweep"): tiles are claimed in order through an atomic
+// counter, each tile publishes its digit counts, and looks back over its
 // predecessors' published words until it finds an inclusive prefix.  Every
 // wait is bounded (kSpinLimit); on expiry the kernel raises
 // kStatusSpinLimit in the caller's status word and carries on with what it
@@ -10,9 +12,9 @@
 //
 // The radix sort is stable (ranks within a warp come from the lanes sharing
 // a digit, found with one ballot per digit bit, over warp-striped items in
-// input order), so equal keys keep their input
-// order exactly as cub::DeviceRadixSort::SortPairs does
-// (CudaQuadTree.cu:405-407), which the Morton permutation parity needs.
+// input order), so equal keys keep their input order exactly as
+// cub::DeviceRadixSort::SortPairs does (CudaQuadTree.cu:405-407), which the
+// Morton permutation parity needs.
 #include "nbx_internal.cuh"
 
 namespace nbx {
@@ -20,38 +22,64 @@ namespace nbx {
 // ------------------------------------------------------------------ scan
 namespace {
 
-constexpr uint64_t kFlagShift = 62;
-constexpr uint64_t kValueMask = (1ull << 62) - 1;
-constexpr uint64_t kFlagAgg = 1ull << kFlagShift;
-constexpr uint64_t kFlagIncl = 2ull << kFlagShift;
+
+// Reduce-then-apply scan: the tile sums first (no dependence between
+// tiles), then every tile adds the sums of the tiles before it (read from
+// L2, summed in shared memory) and scans its items.  Two launches and no
+// look-back chain, whose length grows with the number of tiles.
+__device__ __forceinline__ uint32_t block_sum_u32(uint32_t v, uint32_t *sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  uint32_t t = 0;
+  for (int w = 0; w < kScanThreads / 32; ++w) t += sh[w];
+  return t;
+}
 
 __global__ void __launch_bounds__(kScanThreads)
-    k_scan(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
-           uint32_t n_max, const uint32_t *d_n, uint32_t *total,
-           uint64_t *status, uint32_t *tileCounter, uint32_t *err) {
-  __shared__ uint32_t s_tile;
+    k_scan_reduce(const uint32_t *__restrict__ in, uint32_t n_max, const uint32_t *d_n,
+                  uint32_t *__restrict__ tileSum) {
+  __shared__ uint32_t sh[kScanThreads / 32];
+  const uint32_t n = load_count(d_n, n_max);
+  const uint32_t base = blockIdx.x * kScanTile;
+  if (base >= n) return;
+  uint32_t v = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const uint32_t i = base + k * kScanThreads + threadIdx.x;
+    if (i < n) v += in[i];
+  }
+  const uint32_t t = block_sum_u32(v, sh);
+  if (threadIdx.x == 0) tileSum[blockIdx.x] = t;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan_apply(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
+                 uint32_t n_max, const uint32_t *d_n, uint32_t *total,
+                 const uint32_t *__restrict__ tileSum) {
   __shared__ uint32_t s_items[kScanTile];
   __shared__ uint32_t s_warp[kScanThreads / 32];
-  __shared__ uint64_t s_excl;
+  __shared__ uint32_t sh[kScanThreads / 32];
   const int tid = threadIdx.x;
   const uint32_t n = load_count(d_n, n_max);
   const uint32_t numTiles = (n + kScanTile - 1) / kScanTile;
-  if (tid == 0) s_tile = atomicAdd(tileCounter, 1u);
-  __syncthreads();
-  const uint32_t tile = s_tile;
+  const uint32_t tile = blockIdx.x;
   if (n == 0) {
     if (tile == 0 && tid == 0 && total) *total = 0;
     return;
   }
   if (tile >= numTiles) return;
+  uint32_t pre = 0;
+  for (uint32_t t = tid; t < tile; t += kScanThreads) pre += tileSum[t];
+  const uint32_t excl = block_sum_u32(pre, sh);
   const uint32_t base = tile * kScanTile;
-  // striped, coalesced load into shared memory
   for (int k = 0; k < kScanItems; ++k) {
     const uint32_t i = base + k * kScanThreads + tid;
     s_items[k * kScanThreads + tid] = i < n ? in[i] : 0u;
   }
   __syncthreads();
-  // blocked read: thread tid owns items [tid*16, tid*16+16)
   uint32_t v[kScanItems];
   uint32_t sum = 0;
 #pragma unroll
@@ -59,7 +87,6 @@ __global__ void __launch_bounds__(kScanThreads)
     v[k] = s_items[tid * kScanItems + k];
     sum += v[k];
   }
-  // warp inclusive scan of per-thread sums
   const int lane = tid & 31, warp = tid >> 5;
   uint32_t inc = sum;
 #pragma unroll
@@ -69,57 +96,14 @@ __global__ void __launch_bounds__(kScanThreads)
   }
   if (lane == 31) s_warp[warp] = inc;
   __syncthreads();
-  if (warp == 0) {
-    uint32_t w = lane < kScanThreads / 32 ? s_warp[lane] : 0u;
-    uint32_t wi = w;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
-      if (lane >= o) wi += t;
-    }
-    const uint32_t blockTotal = __shfl_sync(0xffffffffu, wi, kScanThreads / 32 - 1);
-    if (lane < kScanThreads / 32) s_warp[lane] = wi - w; // exclusive
-    uint32_t excl = 0;
-    if (tile == 0) {
-      if (lane == 0) st_relaxed_u64(&status[0], kFlagIncl | (uint64_t)blockTotal);
-    } else {
-      if (lane == 0) st_relaxed_u64(&status[tile], kFlagAgg | (uint64_t)blockTotal);
-      // warp-wide look-back: lane j reads predecessor pred - j, so one
-      // round trip covers 32 predecessors; the nearest inclusive prefix
-      // ends the walk, aggregates before it are summed
-      int64_t pred = (int64_t)tile - 1;
-      uint32_t spins = 0;
-      for (;;) {
-        const int64_t p = pred - lane;
-        const uint64_t st = p >= 0 ? ld_relaxed_u64(&status[p]) : kFlagIncl;
-        const uint32_t flag = (uint32_t)(st >> kFlagShift);
-        const uint32_t inclMask = __ballot_sync(0xffffffffu, flag == 2u);
-        const uint32_t zeroMask = __ballot_sync(0xffffffffu, flag == 0u);
-        const int firstIncl = inclMask ? __ffs(inclMask) - 1 : 32;
-        const int firstZero = zeroMask ? __ffs(zeroMask) - 1 : 32;
-        // lanes up to and including the prefix, or up to the first gap
-        const int take = firstIncl < firstZero ? firstIncl + 1 : firstZero;
-        excl += __reduce_add_sync(0xffffffffu, lane < take ? (uint32_t)(st & kValueMask) : 0u);
-        if (firstIncl < firstZero) break; // reached an inclusive prefix
-        pred -= take;
-        if (take == 0) {
-          if (++spins > kSpinLimit) {
-            if (lane == 0) atomicOr(err, kStatusSpinLimit);
-            break;
-          }
-          __nanosleep(64);
-        }
-      }
-      if (lane == 0)
-        st_relaxed_u64(&status[tile], kFlagIncl | ((uint64_t)(excl + blockTotal) & kValueMask));
-    }
-    if (lane == 0) {
-      s_excl = excl;
-      if (total && tile == numTiles - 1) *total = (uint32_t)(excl + blockTotal);
-    }
+  uint32_t woff = 0, blockTotal = 0;
+  for (int w = 0; w < kScanThreads / 32; ++w) {
+    if (w < warp) woff += s_warp[w];
+    blockTotal += s_warp[w];
   }
+  if (total && tile == numTiles - 1 && tid == 0) *total = excl + blockTotal;
+  uint32_t run = excl + woff + (inc - sum);
   __syncthreads();
-  uint32_t run = (uint32_t)s_excl + s_warp[warp] + (inc - sum);
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
     s_items[tid * kScanItems + k] = run;
@@ -142,10 +126,11 @@ void exclusive_scan_u32(cudaStream_t s, const uint32_t *in, uint32_t *out,
                         uint32_t n_max, const uint32_t *d_n, uint32_t *total,
                         ScanScratch &sc, uint32_t *err) {
   const uint32_t tiles = (n_max + kScanTile - 1) / kScanTile;
-  cudaMemsetAsync(sc.status, 0, sizeof(uint64_t) * (tiles + 1), s);
-  cudaMemsetAsync(sc.tileCounter, 0, sizeof(uint32_t), s);
-  k_scan<<<tiles > 0 ? tiles : 1, kScanThreads, 0, s>>>(
-      in, out, n_max, d_n, total, sc.status, sc.tileCounter, err);
+  uint32_t *tileSum = reinterpret_cast<uint32_t *>(sc.status);
+  (void)err;
+  k_scan_reduce<<<tiles > 0 ? tiles : 1, kScanThreads, 0, s>>>(in, n_max, d_n, tileSum);
+  k_scan_apply<<<tiles > 0 ? tiles : 1, kScanThreads, 0, s>>>(in, out, n_max, d_n, total,
+                                                               tileSum);
 }
 
 // ------------------------------------------------------------ radix sort
