@@ -26,7 +26,7 @@ void launch_bounds(cudaStream_t s, const DevState &S);
 void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
                   SortScratch &sort);
 void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
-                   const MlpDev *mlp, float band, int corr);
+                   const MlpDev *mlp, float band, int corr, bool noClamp);
 void render_vertices(cudaStream_t s, const float4 *pv, const float2 *mr, uint32_t n,
                      const RenderParams &P, float4 *v0, float4 *v1, uint32_t *tiles,
                      double4 *partial, unsigned long long *total, float *stats);
@@ -73,8 +73,12 @@ using namespace nbx;
 
 namespace {
 
+// Unpacks body records; *maxMassBits receives the largest |mass| as float
+// bits (non-negative floats order as their bit patterns; NaN orders last).
 __global__ void k_unpack(const nbx_body *__restrict__ in, uint32_t n,
-                         float4 *pv, float2 *acc, float2 *mr, uint32_t *id) {
+                         float4 *pv, float2 *acc, float2 *mr, uint32_t *id,
+                         uint32_t *maxMassBits) {
+  uint32_t mb = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += gridDim.x * blockDim.x) {
     const nbx_body b = in[i];
@@ -82,7 +86,10 @@ __global__ void k_unpack(const nbx_body *__restrict__ in, uint32_t n,
     acc[i] = make_float2(b.acc_x, b.acc_y);
     mr[i] = make_float2(b.mass, b.radius);
     id[i] = b.id;
+    mb = max(mb, __float_as_uint(b.mass) & 0x7fffffffu);
   }
+  mb = __reduce_max_sync(0xffffffffu, mb);
+  if ((threadIdx.x & 31) == 0 && mb) atomicMax(maxMassBits, mb);
 }
 
 // NBS2 frame record in id order: {x, y, vx, vy} = the body's pv record.
@@ -236,6 +243,7 @@ struct nbx_handle {
   // attractor (CudaSimulation.cuh:9-15 defaults): {x, y, mass, softening},
   // {active, 0, 0, 0}; mirrored into S.attr
   float attrHost[8] = {0.0f, 0.0f, 1e6f, 50.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  float maxAbsMass = INFINITY; // largest |mass| of the uploaded bodies
   FrameWriter *frames = nullptr; // created by the first nbx_nbs2_record
   // splat renderer buffers, grown on demand
   struct {
@@ -442,6 +450,16 @@ void sync_params(nbx_handle *h) {
   S.collisions = P.collisions;
 }
 
+// Whether the default force law can leave out its FLT_MAX clamp: the factor
+// m * fastInvSqrt(d^2) / (d^2 + eps^2) stays below FLT_MAX (fastInvSqrt <=
+// ~2e19) for eps > 0 and |m| < 1.6e19 * min(1, eps^2); NaN masses keep it.
+bool forces_unclamped(const nbx_handle *h) {
+  const nbx_params &P = h->params;
+  const float eSq = P.epsilon * P.epsilon;
+  return !P.exact_math && P.use_mlp == 0 && eSq > 0.0f &&
+         h->maxAbsMass < 1.6e19f * fminf(1.0f, eSq);
+}
+
 // One Simulation::step on stream s for state S; returns the state after the
 // Morton gather's buffer swap.
 DevState enqueue_step(nbx_handle *h, cudaStream_t s, DevState S) {
@@ -465,7 +483,7 @@ DevState enqueue_step(nbx_handle *h, cudaStream_t s, DevState S) {
   if (h->timedCapture) cudaEventRecordWithFlags(h->forceMark[0], s, cudaEventRecordExternal);
   launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
                 h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
-                h->params.use_mlp);
+                h->params.use_mlp, forces_unclamped(h));
   if (h->timedCapture) cudaEventRecordWithFlags(h->forceMark[1], s, cudaEventRecordExternal);
   mark(s, "forces");
   return S;
@@ -723,14 +741,27 @@ int nbx_upload_bodies(nbx_handle *h, const nbx_body *bodies, size_t n) {
   NBX_CUDA(h, cudaMemcpyAsync(h->dAoS, src, n * sizeof(nbx_body),
                               cudaMemcpyHostToDevice, h->stream));
   const DevState S = h->state();
+  NBX_CUDA(h, cudaMemsetAsync(S.counters + 12, 0, sizeof(uint32_t), h->stream));
   k_unpack<<<std::min<uint32_t>((h->n + 255) / 256, 4096), 256, 0, h->stream>>>(
-      h->dAoS, h->n, S.pv, S.acc, S.mr, S.id);
+      h->dAoS, h->n, S.pv, S.acc, S.mr, S.id, S.counters + 12);
   NBX_CUDA(h, cudaGetLastError());
+  uint32_t massBits = 0;
+  NBX_CUDA(h, cudaMemcpyAsync(&massBits, S.counters + 12, sizeof(uint32_t),
+                              cudaMemcpyDeviceToHost, h->stream));
   // collision cell per instance: 2 x median radius x 1.01 (CudaCollision.cu:201-215)
   std::vector<SegDev> seg(h->nseg);
   NBX_CUDA(h, cudaMemcpyAsync(seg.data(), S.seg, h->nseg * sizeof(SegDev),
                               cudaMemcpyDeviceToHost, h->stream));
   NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  {
+    // the force pass leaves out its FLT_MAX clamp when it cannot act; a
+    // change of that choice needs new step graphs
+    const bool before = forces_unclamped(h);
+    float mm;
+    std::memcpy(&mm, &massBits, sizeof(mm));
+    h->maxAbsMass = mm;
+    if (forces_unclamped(h) != before) destroy_graphs(h);
+  }
   // The grid cell only sets how the broadphase partitions space: the
   // candidate set (every overlapping box pair) does not depend on it.  It
   // is 2 x 1.01 x the median radius of an evenly strided sample of at most
@@ -1226,7 +1257,7 @@ int nbx_phase(nbx_handle *h, int phase) {
     if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
     launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
                   h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
-                  h->params.use_mlp);
+                  h->params.use_mlp, forces_unclamped(h));
     break;
   case NBX_PHASE_ATTRACT:
     if (h->params.force_law == 1) {
@@ -1243,7 +1274,7 @@ int nbx_phase(nbx_handle *h, int phase) {
     h->forceInput = true;
     launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
                   h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
-                  h->params.use_mlp);
+                  h->params.use_mlp, forces_unclamped(h));
     break;
   case NBX_PHASE_STEP:
     enqueue_step(h, s, S);

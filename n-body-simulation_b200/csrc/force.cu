@@ -51,18 +51,22 @@ __device__ __forceinline__ float inv_sqrt_law(float x) {
 }
 
 // The tree force law's factor m * fastInvSqrt(d^2) / (d^2 + eps^2), clamped
-// to FLT_MAX (the term is d * factor).
-template <bool kExact>
+// to FLT_MAX (the term is d * factor).  kClamp = false leaves the clamp out
+// where it cannot act: fastInvSqrt never exceeds ~2e19 (its value at 0), so
+// with eps > 0 and every |m| < 1.6e19 * min(1, eps^2) neither m * fastInvSqrt
+// nor the factor reaches FLT_MAX (the host checks this before choosing it).
+template <bool kExact, bool kClamp = true>
 __device__ __forceinline__ float law_factor(float dSq, float m, float eSq) {
   if (kExact)
     return fminf(__fmul_rn(__fmul_rn(m, inv_sqrt_law<true>(dSq)),
                            __frcp_rn(__fadd_rn(dSq, eSq))),
                  FLT_MAX);
-  return fminf(m * inv_sqrt_law<false>(dSq) * rcp_approx(dSq + eSq), FLT_MAX);
+  const float f = m * inv_sqrt_law<false>(dSq) * rcp_approx(dSq + eSq);
+  return kClamp ? fminf(f, FLT_MAX) : f;
 }
 
 // One interaction of the tree force law; accumulates into (ax, ay).
-template <bool kExact>
+template <bool kExact, bool kClamp = true>
 __device__ __forceinline__ void add_term(float dx, float dy, float dSq,
                                          float m, float eSq, float &ax,
                                          float &ay) {
@@ -73,8 +77,7 @@ __device__ __forceinline__ void add_term(float dx, float dy, float dSq,
     ax = __fadd_rn(ax, __fmul_rn(dx, f));
     ay = __fadd_rn(ay, __fmul_rn(dy, f));
   } else {
-    const float f =
-        fminf(m * inv_sqrt_law<false>(dSq) * rcp_approx(dSq + eSq), FLT_MAX);
+    const float f = law_factor<false, kClamp>(dSq, m, eSq);
     ax = fmaf(dx, f, ax);
     ay = fmaf(dy, f, ay);
   }
@@ -116,7 +119,7 @@ __device__ __forceinline__ void quad_term(float dx, float dy, float dSq,
 // kCorr = 1: accepted cells with size^2 >= d^2 * band^2 get the learned
 // correction (mlp.cuh), evaluated for the warp's rows on tensor cores;
 // kCorr = 2: they get the analytic quadrupole term instead (the control).
-template <bool kExact, bool kCount = false, int kCorr = 0>
+template <bool kExact, bool kCount = false, int kCorr = 0, bool kClamp = true>
 __global__ void __launch_bounds__(kForceBlock)
     k_forces(DevState S, float tSq, float eSq,
              unsigned long long *counts = nullptr,
@@ -176,7 +179,7 @@ __global__ void __launch_bounds__(kForceBlock)
       const bool openLeaf = at && !accept && B.w != 0;
       {
         const bool use = accept && A.z > 0.0f;
-        const float fac = law_factor<kExact>(dSq, A.z, eSq);
+        const float fac = law_factor<kExact, kClamp>(dSq, A.z, eSq);
         float tx, ty;
         if (kExact) {
           tx = __fadd_rn(ax, __fmul_rn(dx, fac));
@@ -240,7 +243,7 @@ __global__ void __launch_bounds__(kForceBlock)
             const float ex = kExact ? __fsub_rn(q.x, x) : q.x - x;
             const float ey = kExact ? __fsub_rn(q.y, y) : q.y - y;
             float tx = ax, ty = ay;
-            add_term<kExact>(ex, ey, sq_dist<kExact>(ex, ey), q.z, eSq, tx, ty);
+            add_term<kExact, kClamp>(ex, ey, sq_dist<kExact>(ex, ey), q.z, eSq, tx, ty);
             ax = openLeaf ? tx : ax;
             ay = openLeaf ? ty : ay;
           }
@@ -341,7 +344,7 @@ void launch_query_forces(cudaStream_t s, const DevState &S, bool exact,
 }
 
 void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
-                   const MlpDev *mlp, float band, int corr) {
+                   const MlpDev *mlp, float band, int corr, bool noClamp) {
   if (blocks <= 0) {
     uint32_t warps = (S.n + 31) / 32;
     uint32_t b = (warps + kWarps - 1) / kWarps;
@@ -355,6 +358,8 @@ void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
         S, S.tSq, S.eSq, nullptr, nullptr, band * band, sqrtf(S.eSq));
   else if (exact)
     k_forces<true><<<blocks, kForceBlock, 0, s>>>(S, S.tSq, S.eSq);
+  else if (noClamp)
+    k_forces<false, false, 0, false><<<blocks, kForceBlock, 0, s>>>(S, S.tSq, S.eSq);
   else
     k_forces<false><<<blocks, kForceBlock, 0, s>>>(S, S.tSq, S.eSq);
 }

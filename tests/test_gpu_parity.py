@@ -336,3 +336,23 @@ def test_capacity_errors_reported(nbx, oracle):
         sim.phase("collide")
     assert e.value.code == 3
     sim.close()
+
+
+@pytest.mark.parametrize("mass,eps", [(1e30, 1.0), (2e19, 1.0), (1e6, 1e-3), (1.0, 0.0)])
+def test_force_clamp_kept_where_it_can_act(nbx, oracle, mass, eps):
+    """The default force pass leaves out the FLT_MAX clamp of the force law
+    only where it cannot act (eps > 0 and every |m| < 1.6e19 min(1, eps^2));
+    with a huge mass or tiny softening the clamp stays and the forces agree
+    with the reference's clamped law."""
+    b = nbx.uniform_disc(5000)
+    b["mass"][0] = np.float32(mass)
+    _, _, _, sb, tree = oracle.morton_build(b)
+    ox, oy = oracle.tree_forces(sb["px"], sb["py"], sb["mass"], tree, 0.5, eps)
+    sim = nbx.Simulation(b, theta=0.5, epsilon=eps)
+    sim.phase("attract")
+    g = sim.download()
+    fin = np.isfinite(ox) & np.isfinite(oy)
+    assert np.array_equal(np.isfinite(g["ax"]) & np.isfinite(g["ay"]), fin)
+    e = rel_err(g["ax"][fin], g["ay"][fin], ox[fin], oy[fin])
+    assert np.percentile(e, 99) < 1e-5 and e.max() < 1e-4, (np.percentile(e, 99), e.max())
+    sim.close()
