@@ -450,13 +450,14 @@ void sync_params(nbx_handle *h) {
   S.collisions = P.collisions;
 }
 
-// Whether the default force law can leave out its FLT_MAX clamp: the factor
+// Whether the default force law (plain or with the quadrupole term) can
+// leave out its FLT_MAX clamp: the factor
 // m * fastInvSqrt(d^2) / (d^2 + eps^2) stays below FLT_MAX (fastInvSqrt <=
 // ~2e19) for eps > 0 and |m| < 1.6e19 * min(1, eps^2); NaN masses keep it.
 bool forces_unclamped(const nbx_handle *h) {
   const nbx_params &P = h->params;
   const float eSq = P.epsilon * P.epsilon;
-  return !P.exact_math && P.use_mlp == 0 && eSq > 0.0f &&
+  return !P.exact_math && P.use_mlp != 1 && eSq > 0.0f &&
          h->maxAbsMass < 1.6e19f * fminf(1.0f, eSq);
 }
 

@@ -353,6 +353,9 @@ void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
   if (corr == 1 && mlp)
     k_forces<false, false, 1><<<blocks, kForceBlock, 0, s>>>(
         S, S.tSq, S.eSq, nullptr, mlp, band * band, sqrtf(S.eSq));
+  else if (corr == 2 && noClamp)
+    k_forces<false, false, 2, false><<<blocks, kForceBlock, 0, s>>>(
+        S, S.tSq, S.eSq, nullptr, nullptr, band * band, sqrtf(S.eSq));
   else if (corr == 2)
     k_forces<false, false, 2><<<blocks, kForceBlock, 0, s>>>(
         S, S.tSq, S.eSq, nullptr, nullptr, band * band, sqrtf(S.eSq));
