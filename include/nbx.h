@@ -251,6 +251,14 @@ int nbx_nbs2_record(nbx_handle *h, nbx_nbs2 *f);
 /* Waits until every recorded frame is written; returns the first error. */
 int nbx_nbs2_flush(nbx_handle *h);
 
+/* Failure detection check: enqueues one bounded device wait on a flag that
+ * nothing sets -- the same loop, limit and status bit as the ordered
+ * resolution's and the radix sort's waits -- so that the next nbx_sync
+ * returns NBX_ERR_TIMEOUT (about a second later) and the handle stays usable
+ * afterwards.  No counterpart in the reference, whose waits are
+ * unbounded. */
+int nbx_debug_expire_wait(nbx_handle *h);
+
 /* --- FP64 checks --- */
 
 /* FP64 direct-sum accelerations for bodies at the given current indices,

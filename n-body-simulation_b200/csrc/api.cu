@@ -92,6 +92,21 @@ __global__ void k_unpack(const nbx_body *__restrict__ in, uint32_t n,
   if ((threadIdx.x & 31) == 0 && mb) atomicMax(maxMassBits, mb);
 }
 
+// A bounded wait on a flag that nothing sets, shaped like the waits of the
+// ordered resolution and the sort look-back (poll, back off, give up after
+// kSpinLimit rounds and raise kStatusSpinLimit).
+__global__ void k_expire_wait(const uint32_t *flag, uint32_t *status) {
+  uint32_t idle = 0;
+  for (;;) {
+    if (ld_acquire_u32(flag) != 0u) return;
+    if (++idle > kSpinLimit) {
+      if (threadIdx.x == 0) atomicOr(status, kStatusSpinLimit);
+      return;
+    }
+    __nanosleep(32);
+  }
+}
+
 // NBS2 frame record in id order: {x, y, vx, vy} = the body's pv record.
 __global__ void k_frame_scatter(const float4 *__restrict__ pv,
                                 const uint32_t *__restrict__ id, uint32_t n,
@@ -1209,6 +1224,16 @@ int nbx_reset(nbx_handle *h, const nbx_body *bodies, size_t n) {
   if (!mlp.empty() && (rc = nbx_mlp_set_params(h, mlp.data(), kMlpParams)) != NBX_OK)
     return rc;
   return nbx_upload_bodies(h, bodies, n);
+}
+
+int nbx_debug_expire_wait(nbx_handle *h) {
+  if (!h) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  uint32_t *flag = h->base.counters + 13; // never set
+  NBX_CUDA(h, cudaMemsetAsync(flag, 0, sizeof(uint32_t), h->stream));
+  k_expire_wait<<<1, 32, 0, h->stream>>>(flag, h->base.status);
+  NBX_CUDA(h, cudaGetLastError());
+  return NBX_OK;
 }
 
 int nbx_sync(nbx_handle *h) {

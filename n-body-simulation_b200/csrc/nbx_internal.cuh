@@ -18,9 +18,10 @@ enum StatusBits : uint32_t {
   kStatusBadSegment = 1u << 5,
 };
 
-// Iteration cap of every spin-wait in this library (each iteration sleeps
-// ~64-256 ns, so this bounds a wait at well under a few seconds).
-constexpr uint32_t kSpinLimit = 1u << 23;
+// Iteration cap of every spin-wait in this library: each round polls memory
+// (an L2 round trip) and backs off, so a wait gives up after about a
+// second; legitimate waits here last microseconds.
+constexpr uint32_t kSpinLimit = 1u << 21;
 
 __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
   uint32_t v;

@@ -40,7 +40,7 @@ EXPORTS = (
     "nbx_make_scenario", "nbx_renumber", "nbx_add_heavy_body", "nbx_add_cluster",
     "nbx_set_attractor", "nbx_reset", "nbx_nbs2_record", "nbx_nbs2_flush",
     "nbx_nbs2_open", "nbx_nbs2_write_packed", "nbx_nbs2_close",
-    "nbx_draw_default", "nbx_render", "nbx_body_stats",
+    "nbx_draw_default", "nbx_render", "nbx_body_stats", "nbx_debug_expire_wait",
 )
 SCENARIOS = {"disc": 0, "two_galaxies": 1, "cold_square": 2}
 MLP_PARAMS = 1442
@@ -116,6 +116,7 @@ def lib() -> C.CDLL:
         "nbx_render": [vp, C.POINTER(Camera), C.POINTER(Draw), C.c_uint32, C.c_uint32,
                        vp, vp],
         "nbx_body_stats": [vp, vp],
+        "nbx_debug_expire_wait": [vp],
         "nbx_reset": [vp, vp, C.c_size_t],
         "nbx_sync": [vp],
         "nbx_phase": [vp, C.c_int],

@@ -319,6 +319,23 @@ def test_nonfinite_reported(nbx):
     sim.close()
 
 
+def test_bounded_wait_expires_and_handle_recovers(nbx):
+    """A device wait that nothing completes ends by its own bound (no fault,
+    no hang): the host sees NBX_ERR_TIMEOUT and the handle keeps working."""
+    import time
+    sim = nbx.Simulation(nbx.uniform_disc(2000))
+    t0 = time.perf_counter()
+    sim._c(nbx.lib().nbx_debug_expire_wait(sim.h))
+    with pytest.raises(nbx.NbxError) as e:
+        sim.sync()
+    assert e.value.code == 5  # NBX_ERR_TIMEOUT
+    assert time.perf_counter() - t0 < 60
+    sim.step(3)
+    sim.sync()
+    assert np.isfinite(sim.download()["px"]).all()
+    sim.close()
+
+
 def test_capacity_errors_reported(nbx, oracle):
     b = nbx.uniform_disc(20000)
     sim = nbx.Simulation(b, node_factor=0.01)
