@@ -131,3 +131,24 @@ def test_nbs2_writer(nbx, tmp_path):
     assert np.array_equal(mass, b["mass"]) and np.array_equal(radius, b["radius"])
     assert np.array_equal(frames[1][:, 0], written[1]["px"])
     assert np.array_equal(frames[0][:, 2], written[0]["vx"])
+
+
+def test_draw_defaults_are_the_viewers(nbx):
+    """DrawSettings defaults (viewer/Renderer.h:14-20); no GPU needed."""
+    d = nbx.Draw()
+    nbx.lib().nbx_draw_default(nbx.C.byref(d))
+    assert (d.mode, d.point_scale, d.min_point_px) == (1, 1.0, 1.5)
+    assert abs(d.brightness - 0.6) < 1e-7 and d.speed_max == 60.0
+
+
+def test_scenario_arguments_checked(nbx):
+    with pytest.raises(nbx.NbxError):
+        nbx.make_scenario("disc", 0)
+    with pytest.raises(nbx.NbxError):
+        nbx.make_scenario("two_galaxies", 1)
+    assert nbx.lib().nbx_make_scenario(7, 10, 0, None) != 0  # unknown kind
+    b = nbx.make_scenario("cold_square", 5000, 2)
+    assert np.array_equal(b["id"], np.arange(5000)) and (b["mass"] == 1).all()
+    h = 3.0 * np.sqrt(5000)
+    assert np.abs(b["px"]).max() <= h and np.abs(b["py"]).max() <= h
+    assert nbx.cold_square(5000, 2).tobytes() == b.tobytes()
