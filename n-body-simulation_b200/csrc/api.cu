@@ -5,6 +5,7 @@
 #include "nbx_state.cuh"
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <condition_variable>
 #include <deque>
@@ -86,7 +87,9 @@ __global__ void k_unpack(const nbx_body *__restrict__ in, uint32_t n,
     acc[i] = make_float2(b.acc_x, b.acc_y);
     mr[i] = make_float2(b.mass, b.radius);
     id[i] = b.id;
-    mb = max(mb, __float_as_uint(b.mass) & 0x7fffffffu);
+    // bit order = value order for non-negative floats; any negative mass
+    // (sign bit set) lands above every non-negative one
+    mb = max(mb, __float_as_uint(b.mass));
   }
   mb = __reduce_max_sync(0xffffffffu, mb);
   if ((threadIdx.x & 31) == 0 && mb) atomicMax(maxMassBits, mb);
@@ -258,7 +261,7 @@ struct nbx_handle {
   // attractor (CudaSimulation.cuh:9-15 defaults): {x, y, mass, softening},
   // {active, 0, 0, 0}; mirrored into S.attr
   float attrHost[8] = {0.0f, 0.0f, 1e6f, 50.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-  float maxAbsMass = INFINITY; // largest |mass| of the uploaded bodies
+  float maxMass = INFINITY; // largest uploaded mass; +inf if any is negative
   FrameWriter *frames = nullptr; // created by the first nbx_nbs2_record
   // splat renderer buffers, grown on demand
   struct {
@@ -468,12 +471,15 @@ void sync_params(nbx_handle *h) {
 // Whether the default force law (plain or with the quadrupole term) can
 // leave out its FLT_MAX clamp: the factor
 // m * fastInvSqrt(d^2) / (d^2 + eps^2) stays below FLT_MAX (fastInvSqrt <=
-// ~2e19) for eps > 0 and |m| < 1.6e19 * min(1, eps^2); NaN masses keep it.
+// ~2e19 for finite d^2) for a normal eps^2 and masses in
+// [0, 1.6e19 * min(1, eps^2)); NaN or negative masses keep it.  Non-negative
+// masses keep every centre of mass inside its bodies' box, and the build's
+// per-instance coordinate check (SegDev::wide) keeps d^2 finite.
 bool forces_unclamped(const nbx_handle *h) {
   const nbx_params &P = h->params;
   const float eSq = P.epsilon * P.epsilon;
-  return !P.exact_math && P.use_mlp != 1 && eSq > 0.0f &&
-         h->maxAbsMass < 1.6e19f * fminf(1.0f, eSq);
+  return !P.exact_math && P.use_mlp != 1 && eSq >= FLT_MIN &&
+         h->maxMass < 1.6e19f * fminf(1.0f, eSq);
 }
 
 // One Simulation::step on stream s for state S; returns the state after the
@@ -769,14 +775,21 @@ int nbx_upload_bodies(nbx_handle *h, const nbx_body *bodies, size_t n) {
   NBX_CUDA(h, cudaMemcpyAsync(seg.data(), S.seg, h->nseg * sizeof(SegDev),
                               cudaMemcpyDeviceToHost, h->stream));
   NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  // the force pass leaves out its FLT_MAX clamp when it cannot act; a
+  // change of that choice needs new step graphs
+  uint32_t coordLimitBits = 0;
   {
-    // the force pass leaves out its FLT_MAX clamp when it cannot act; a
-    // change of that choice needs new step graphs
     const bool before = forces_unclamped(h);
-    float mm;
-    std::memcpy(&mm, &massBits, sizeof(mm));
-    h->maxAbsMass = mm;
+    float mm = INFINITY; // a negative mass (or -0): keep the clamp
+    if (!(massBits & 0x80000000u)) std::memcpy(&mm, &massBits, sizeof(mm));
+    h->maxMass = mm;
     if (forces_unclamped(h) != before) destroy_graphs(h);
+    // every node sum of x * m stays below 1e36 and every distance below
+    // 1.2e19 (its square finite) while all |x|, |y| < this limit
+    float lim = 4e18f;
+    if (mm > 0.0f && std::isfinite(mm))
+      lim = std::fmin(lim, 1e36f / (static_cast<float>(h->n) * mm));
+    std::memcpy(&coordLimitBits, &lim, sizeof(lim));
   }
   // The grid cell only sets how the broadphase partitions space: the
   // candidate set (every overlapping box pair) does not depend on it.  It
@@ -802,6 +815,8 @@ int nbx_upload_bodies(nbx_handle *h, const nbx_body *bodies, size_t n) {
   }
   NBX_CUDA(h, cudaMemcpyAsync(S.seg, seg.data(), h->nseg * sizeof(SegDev),
                               cudaMemcpyHostToDevice, h->stream));
+  NBX_CUDA(h, cudaMemcpyAsync(S.counters + kCtrCoordLimit, &coordLimitBits,
+                              sizeof(coordLimitBits), cudaMemcpyHostToDevice, h->stream));
   NBX_CUDA(h, cudaStreamSynchronize(h->stream));
   h->idsChecked = false;
   h->uploaded = true;

@@ -65,6 +65,10 @@ __global__ void k_root_frame(DevState S) {
   G.cy = cy;
   G.size = size;
   G.frame = sd_morton_frame(cx, cy, size);
+  // clamp guard: bodies beyond the upload's coordinate limit (NaN-safe)
+  const float lim = __uint_as_float(S.counters[kCtrCoordLimit]);
+  const float reach = fmaxf(fmaxf(fabsf(minX), fabsf(maxX)), fmaxf(fabsf(minY), fabsf(maxY)));
+  G.wide = (b[0] != 0xffffffffu && !(reach < lim)) ? 1u : 0u;
   b[0] = 0xffffffffu;
   b[1] = 0u;
   b[2] = 0xffffffffu;

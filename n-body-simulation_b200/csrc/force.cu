@@ -116,24 +116,118 @@ __device__ __forceinline__ void quad_term(float dx, float dy, float dSq,
   qy = h * (aOverG * (2.0f * Idy + tr * dy) + bOverG * dy * dId);
 }
 
+// One warp's walk: lane targets (x, y) start at node cur (kDone: none) and
+// add their terms to (ax, ay); kCount adds the walk's counts instead.
 // kCorr = 1: accepted cells with size^2 >= d^2 * band^2 get the learned
 // correction (mlp.cuh), evaluated for the warp's rows on tensor cores;
 // kCorr = 2: they get the analytic quadrupole term instead (the control).
-template <bool kExact, bool kCount = false, int kCorr = 0, bool kClamp = true>
-__global__ void __launch_bounds__(kForceBlock)
-    k_forces(DevState S, float tSq, float eSq,
-             unsigned long long *counts = nullptr,
-             const MlpDev *__restrict__ mlp = nullptr, float bandSq = 0.0f,
-             float eps = 0.0f, const float2 *__restrict__ query = nullptr,
-             uint32_t nQuery = 0, float2 *__restrict__ queryAcc = nullptr) {
-  __shared__ float4 sBody[kWarps][32];
-  __shared__ MlpDev sW;
-  __shared__ __nv_bfloat16 sStage[kCorr == 1 ? kWarps : 1][32][16];
-  if (kCorr == 1) {
-    for (int q = threadIdx.x; q < (int)(sizeof(MlpDev) / 4); q += blockDim.x)
-      reinterpret_cast<uint32_t *>(&sW)[q] = reinterpret_cast<const uint32_t *>(mlp)[q];
-    __syncthreads();
+template <bool kExact, bool kCount, int kCorr, bool kClamp>
+__device__ __forceinline__ void walk_targets(
+    const DevState &S, float tSq, float eSq, float bandSq, float eps, float x, float y,
+    uint32_t cur, float4 *sBodyW, const MlpDev &sW, __nv_bfloat16 (*sStageW)[16],
+    float &ax, float &ay, uint32_t &nFar, uint32_t &nNear, uint32_t &nVisit,
+    uint32_t &nIter, uint32_t &nChunk) {
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    const uint32_t k = __reduce_min_sync(0xffffffffu, cur);
+    if (k == kDone) break;
+    if (kCount) ++nIter;
+    // k is the same for the whole warp: one broadcast load through L1
+    const float4 A = __ldg(&S.tA[k]);
+    const int4 B = __ldg(&S.tB[k]);
+    // the node after k's subtree (kDone past the instance's last node)
+    const uint32_t nxt = (uint32_t)B.x;
+    // every lane evaluates the node; only the lanes waiting at it use it
+    const bool at = cur == k;
+    const float dx = kExact ? __fsub_rn(A.x, x) : A.x - x;
+    const float dy = kExact ? __fsub_rn(A.y, y) : A.y - y;
+    const float dSq = sq_dist<kExact>(dx, dy);
+    const float far = kExact ? __fmul_rn(dSq, tSq) : dSq * tSq;
+    const bool accept = at && A.w < far;
+    const bool openLeaf = at && !accept && B.w != 0;
+    {
+      const bool use = accept && A.z > 0.0f;
+      const float fac = law_factor<kExact, kClamp>(dSq, A.z, eSq);
+      float tx, ty;
+      if (kExact) {
+        tx = __fadd_rn(ax, __fmul_rn(dx, fac));
+        ty = __fadd_rn(ay, __fmul_rn(dy, fac));
+      } else {
+        tx = fmaf(dx, fac, ax);
+        ty = fmaf(dy, fac, ay);
+      }
+      if (kCorr == 2) {
+        const bool band = use && A.w >= dSq * bandSq;
+        if (__ballot_sync(0xffffffffu, band)) {
+          const float4 M = S.tM[k];
+          float qx, qy;
+          quad_term(dx, dy, dSq, eSq, A.z, M.x, M.y, M.z, qx, qy);
+          if (band) {
+            tx = ax + fac * (dx + qx);
+            ty = ay + fac * (dy + qy);
+          }
+        }
+      }
+      if (kCorr == 1) {
+        const bool band = use && A.w >= dSq * bandSq;
+        if (__ballot_sync(0xffffffffu, band)) {
+          const float4 M = S.tM[k];
+          const float2 Q = S.tC[k];
+          float f[9], ux = 0.0f, uy = 0.0f;
+          bool ok = band && mlp_features(dx, dy, dSq, A.z, M.w, Q.x, Q.y, A.x,
+                                         A.y, M.x, M.y, M.z, 1.0f, eps, f, ux, uy);
+          if (!ok)
+            for (int q = 0; q < 9; ++q) f[q] = 0.0f;
+          float o0, o1;
+          mlp_warp(sW, f, sStageW, o0, o1);
+          if (ok) {
+            // |mono| * ((1 + t0) u + t1 w), w = (-uy, ux)
+            const float r = dSq * rsqrtf(dSq);
+            tx = ax + fac * (dx * (1.0f + o0) - r * o1 * uy);
+            ty = ay + fac * (dy * (1.0f + o0) + r * o1 * ux);
+          }
+        }
+      }
+      ax = use ? tx : ax;
+      ay = use ? ty : ay;
+      if (kCount) nFar += use ? 1u : 0u;
+    }
+    if (kCount) nVisit += at ? 1u : 0u;
+    // accepted or leaf: skip the subtree; interior node: descend
+    cur = (accept || openLeaf) ? nxt : (at ? k + 1 : cur);
+    const uint32_t leafLanes = __ballot_sync(0xffffffffu, openLeaf);
+    if (leafLanes) {
+      const uint32_t b0 = (uint32_t)B.y, b1 = (uint32_t)B.z;
+      const uint32_t bEnd = b1 <= S.n ? b1 : S.n; // defensive bound
+      for (uint32_t base = b0; base < bEnd; base += 32) {
+        const uint32_t cnt = min(32u, bEnd - base);
+        if (kCount) ++nChunk;
+        __syncwarp();
+        if ((uint32_t)lane < cnt) sBodyW[lane] = S.xym[base + lane];
+        __syncwarp();
+#pragma unroll 4
+        for (uint32_t j = 0; j < cnt; ++j) {
+          const float4 q = sBodyW[j];
+          const float ex = kExact ? __fsub_rn(q.x, x) : q.x - x;
+          const float ey = kExact ? __fsub_rn(q.y, y) : q.y - y;
+          float tx = ax, ty = ay;
+          add_term<kExact, kClamp>(ex, ey, sq_dist<kExact>(ex, ey), q.z, eSq, tx, ty);
+          ax = openLeaf ? tx : ax;
+          ay = openLeaf ? ty : ay;
+        }
+      }
+      if (kCount && openLeaf) nNear += bEnd > b0 ? bEnd - b0 : 0u;
+    }
   }
+}
+
+// Every target of the launch, one warp per 32.
+template <bool kExact, bool kCount, int kCorr, bool kClamp>
+__device__ __forceinline__ void forces_walk(
+    const DevState &S, float tSq, float eSq, unsigned long long *counts,
+    float bandSq, float eps, const float2 *__restrict__ query, uint32_t nQuery,
+    float2 *__restrict__ queryAcc, float4 (*sBody)[32], const MlpDev &sW,
+    __nv_bfloat16 (*sStage)[32][16]) {
   const int lane = threadIdx.x & 31;
   const int w = threadIdx.x >> 5;
   const uint32_t warpsTotal = (gridDim.x * blockDim.x) >> 5;
@@ -145,6 +239,7 @@ __global__ void __launch_bounds__(kForceBlock)
     const bool valid = i < nTargets;
     float x = 0.0f, y = 0.0f;
     uint32_t cur = kDone;
+    bool wide = false;
     if (valid) {
       if (query) {
         const float2 q = query[i];
@@ -157,100 +252,20 @@ __global__ void __launch_bounds__(kForceBlock)
       }
       const SegDev &G = S.seg[query ? 0u : S.segOf[i]];
       if (G.travCount > 0) cur = G.nodeBase;
+      wide = G.wide != 0u;
     }
     float ax = 0.0f, ay = 0.0f;
     uint32_t nFar = 0, nNear = 0, nVisit = 0, nIter = 0, nChunk = 0;
-    for (;;) {
-      const uint32_t k = __reduce_min_sync(0xffffffffu, cur);
-      if (k == kDone) break;
-      if (kCount) ++nIter;
-      // k is the same for the whole warp: one broadcast load through L1
-      const float4 A = __ldg(&S.tA[k]);
-      const int4 B = __ldg(&S.tB[k]);
-      // the node after k's subtree (kDone past the instance's last node)
-      const uint32_t nxt = (uint32_t)B.x;
-      // every lane evaluates the node; only the lanes waiting at it use it
-      const bool at = cur == k;
-      const float dx = kExact ? __fsub_rn(A.x, x) : A.x - x;
-      const float dy = kExact ? __fsub_rn(A.y, y) : A.y - y;
-      const float dSq = sq_dist<kExact>(dx, dy);
-      const float far = kExact ? __fmul_rn(dSq, tSq) : dSq * tSq;
-      const bool accept = at && A.w < far;
-      const bool openLeaf = at && !accept && B.w != 0;
-      {
-        const bool use = accept && A.z > 0.0f;
-        const float fac = law_factor<kExact, kClamp>(dSq, A.z, eSq);
-        float tx, ty;
-        if (kExact) {
-          tx = __fadd_rn(ax, __fmul_rn(dx, fac));
-          ty = __fadd_rn(ay, __fmul_rn(dy, fac));
-        } else {
-          tx = fmaf(dx, fac, ax);
-          ty = fmaf(dy, fac, ay);
-        }
-        if (kCorr == 2) {
-          const bool band = use && A.w >= dSq * bandSq;
-          if (__ballot_sync(0xffffffffu, band)) {
-            const float4 M = S.tM[k];
-            float qx, qy;
-            quad_term(dx, dy, dSq, eSq, A.z, M.x, M.y, M.z, qx, qy);
-            if (band) {
-              tx = ax + fac * (dx + qx);
-              ty = ay + fac * (dy + qy);
-            }
-          }
-        }
-        if (kCorr == 1) {
-          const bool band = use && A.w >= dSq * bandSq;
-          if (__ballot_sync(0xffffffffu, band)) {
-            const float4 M = S.tM[k];
-            const float2 Q = S.tC[k];
-            float f[9], ux = 0.0f, uy = 0.0f;
-            bool ok = band && mlp_features(dx, dy, dSq, A.z, M.w, Q.x, Q.y, A.x,
-                                           A.y, M.x, M.y, M.z, 1.0f, eps, f, ux, uy);
-            if (!ok)
-              for (int q = 0; q < 9; ++q) f[q] = 0.0f;
-            float o0, o1;
-            mlp_warp(sW, f, sStage[w], o0, o1);
-            if (ok) {
-              // |mono| * ((1 + t0) u + t1 w), w = (-uy, ux)
-              const float r = dSq * rsqrtf(dSq);
-              tx = ax + fac * (dx * (1.0f + o0) - r * o1 * uy);
-              ty = ay + fac * (dy * (1.0f + o0) + r * o1 * ux);
-            }
-          }
-        }
-        ax = use ? tx : ax;
-        ay = use ? ty : ay;
-        if (kCount) nFar += use ? 1u : 0u;
-      }
-      if (kCount) nVisit += at ? 1u : 0u;
-      // accepted or leaf: skip the subtree; interior node: descend
-      cur = (accept || openLeaf) ? nxt : (at ? k + 1 : cur);
-      const uint32_t leafLanes = __ballot_sync(0xffffffffu, openLeaf);
-      if (leafLanes) {
-        const uint32_t b0 = (uint32_t)B.y, b1 = (uint32_t)B.z;
-        const uint32_t bEnd = b1 <= S.n ? b1 : S.n; // defensive bound
-        for (uint32_t base = b0; base < bEnd; base += 32) {
-          const uint32_t cnt = min(32u, bEnd - base);
-          if (kCount) ++nChunk;
-          __syncwarp();
-          if ((uint32_t)lane < cnt) sBody[w][lane] = S.xym[base + lane];
-          __syncwarp();
-#pragma unroll 4
-          for (uint32_t j = 0; j < cnt; ++j) {
-            const float4 q = sBody[w][j];
-            const float ex = kExact ? __fsub_rn(q.x, x) : q.x - x;
-            const float ey = kExact ? __fsub_rn(q.y, y) : q.y - y;
-            float tx = ax, ty = ay;
-            add_term<kExact, kClamp>(ex, ey, sq_dist<kExact>(ex, ey), q.z, eSq, tx, ty);
-            ax = openLeaf ? tx : ax;
-            ay = openLeaf ? ty : ay;
-          }
-        }
-        if (kCount && openLeaf) nNear += bEnd > b0 ? bEnd - b0 : 0u;
-      }
-    }
+    // the clamp-free law only while no lane's instance reaches beyond the
+    // coordinate limit (the build's per-instance flag)
+    if (!kClamp && __any_sync(0xffffffffu, wide))
+      walk_targets<kExact, kCount, kCorr, true>(S, tSq, eSq, bandSq, eps, x, y, cur,
+                                                sBody[w], sW, sStage[kCorr == 1 ? w : 0],
+                                                ax, ay, nFar, nNear, nVisit, nIter, nChunk);
+    else
+      walk_targets<kExact, kCount, kCorr, kClamp>(S, tSq, eSq, bandSq, eps, x, y, cur,
+                                                  sBody[w], sW, sStage[kCorr == 1 ? w : 0],
+                                                  ax, ay, nFar, nNear, nVisit, nIter, nChunk);
     if (kCount) {
       unsigned long long f = nFar, nn = nNear, v = nVisit;
       for (int o = 16; o > 0; o >>= 1) {
@@ -274,6 +289,31 @@ __global__ void __launch_bounds__(kForceBlock)
       }
     }
   }
+}
+
+// The force pass.  kClamp = false is the clamp-free law (see law_factor),
+// which the host picks only for non-negative masses below its bound; a
+// warp holding a target whose instance reaches beyond the coordinate limit
+// stored at upload (the build's SegDev::wide), where distances could
+// overflow, takes the clamped walk instead.
+template <bool kExact, bool kCount = false, int kCorr = 0, bool kClamp = true>
+__global__ void __launch_bounds__(kForceBlock)
+    k_forces(DevState S, float tSq, float eSq,
+             unsigned long long *counts = nullptr,
+             const MlpDev *__restrict__ mlp = nullptr, float bandSq = 0.0f,
+             float eps = 0.0f, const float2 *__restrict__ query = nullptr,
+             uint32_t nQuery = 0, float2 *__restrict__ queryAcc = nullptr) {
+  constexpr int kStage = kCorr == 1 ? kWarps : 1;
+  __shared__ float4 sBody[kWarps][32];
+  __shared__ MlpDev sW;
+  __shared__ __nv_bfloat16 sStage[kStage][32][16];
+  if (kCorr == 1) {
+    for (int q = threadIdx.x; q < (int)(sizeof(MlpDev) / 4); q += blockDim.x)
+      reinterpret_cast<uint32_t *>(&sW)[q] = reinterpret_cast<const uint32_t *>(mlp)[q];
+    __syncthreads();
+  }
+  forces_walk<kExact, kCount, kCorr, kClamp>(S, tSq, eSq, counts, bandSq, eps, query, nQuery,
+                                             queryAcc, sBody, sW, sStage);
 }
 
 // FMA throughput probe: 8 independent chains per thread.

@@ -10,7 +10,8 @@ struct SegDev {
   uint32_t start, count;       // body range [start, start+count)
   float cell, invCell, smallW; // collision grid cell; boxes wider than
                                // smallW go to the large list
-  uint32_t pad0;
+  uint32_t wide;               // written every step: bodies reach beyond the
+                               // clamp guard's coordinate limit
   // written every step
   float cx, cy, size; // root square (Quad::newContaining)
   uint32_t pad1;
@@ -25,6 +26,13 @@ struct SegDev {
 
 constexpr int kMaxDepth = 32;   // TreeKernels.cuh:29
 constexpr int kLevelSlots = 34; // depths 0..32 plus an end slot
+
+// counters[] slot of the force law's clamp guard.  The force pass may
+// leave out the law's FLT_MAX clamp only while every distance it forms
+// stays finite: the upload stores the largest coordinate allowed here
+// (float bits), and each build marks the instances whose bodies reach
+// beyond it (SegDev::wide), for the force pass to keep the clamp there.
+constexpr int kCtrCoordLimit = 15;
 
 // Everything a step's kernels touch.  All pointers are device pointers.
 struct DevState {
@@ -83,7 +91,8 @@ struct DevState {
   uint32_t *counters;    // [0]=pairs*2 total [1]=units [2]=unit claim
                          // [3]=splitting entries [4]=total nodes
                          // [5]=small-large pairs [8]=id check
-                         // [9]=long Morton runs
+                         // [9]=long Morton runs [12]=upload mass bits
+                         // [13]=expiry test flag [kCtrCoordLimit] (above)
 
   // Morton / sort
   uint64_t *codes; // unsorted codes (kept for the segment passes)

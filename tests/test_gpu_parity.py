@@ -373,3 +373,56 @@ def test_force_clamp_kept_where_it_can_act(nbx, oracle, mass, eps):
     e = rel_err(g["ax"][fin], g["ay"][fin], ox[fin], oy[fin])
     assert np.percentile(e, 99) < 1e-5 and e.max() < 1e-4, (np.percentile(e, 99), e.max())
     sim.close()
+
+
+def _wide(nbx, scale, shift, central=None, negative=False):
+    b = nbx.uniform_disc(5000)
+    b["px"] *= np.float32(scale)
+    b["py"] *= np.float32(scale)
+    b["px"][::2] += np.float32(shift)
+    b["px"][1::2] -= np.float32(shift)
+    if central is not None:
+        b["mass"][0] = np.float32(central)
+    if negative:
+        b["mass"][7] = np.float32(-3.0)
+    return b
+
+
+@pytest.mark.parametrize("case", ["overflowing distances", "mass-coordinate sums",
+                                  "negative mass"])
+def test_force_clamp_guard_wide_frame(nbx, oracle, case):
+    """The clamp-free law needs every distance and centre-of-mass sum to stay
+    finite: bodies beyond the upload's coordinate limit (here 1.5e19 apart,
+    whose squared distances overflow, or x * m sums near 1e36) send the force
+    pass back to the clamped walk, and a negative mass keeps the clamp, so
+    the result is the reference's clamped law even where it gives inf: no
+    NaN where the reference has a number, every infinity with its sign.
+    (Where the reference gets inf - inf = NaN, the default arithmetic's
+    contracted multiply-add, whose product does not round to inf first, may
+    keep the inf; exact_math reproduces the NaN too.)"""
+    b = {"overflowing distances": lambda: _wide(nbx, 4e14, 1.5e19),
+         "mass-coordinate sums": lambda: _wide(nbx, 4e12, 2e15, central=1e18),
+         "negative mass": lambda: _wide(nbx, 1.0, 0.0, negative=True)}[case]()
+    _, _, _, sb, tree = oracle.morton_build(b)
+    ox, oy = oracle.tree_forces(sb["px"], sb["py"], sb["mass"], tree, 0.5, 1.0)
+    sim = nbx.Simulation(b, theta=0.5, epsilon=1.0)
+    sim.phase("attract")
+    g = sim.download()
+    sim.close()
+    for a, o in ((g["ax"], ox), (g["ay"], oy)):
+        num = ~np.isnan(o)
+        assert not np.isnan(a[num]).any()
+        assert np.array_equal(np.isposinf(a[num]), np.isposinf(o[num]))
+        assert np.array_equal(np.isneginf(a[num]), np.isneginf(o[num]))
+        assert not np.isfinite(a[~num]).any()
+    fin = np.isfinite(ox) & np.isfinite(oy)
+    assert fin.any() or case == "overflowing distances"
+    if fin.any():
+        e = rel_err(g["ax"][fin], g["ay"][fin], ox[fin], oy[fin])
+        assert np.percentile(e, 99) < 1e-5 and e.max() < 1e-4, (np.percentile(e, 99), e.max())
+    sim = nbx.Simulation(b, theta=0.5, epsilon=1.0, exact_math=1)
+    sim.phase("attract")
+    g = sim.download()
+    sim.close()
+    assert np.array_equal(g["ax"], ox, equal_nan=True)
+    assert np.array_equal(g["ay"], oy, equal_nan=True)
