@@ -399,8 +399,7 @@ int allocate(nbx_handle *h) {
   A(S.moments, nodes);
   A(S.subtree, nodes);
   A(S.arrive, nodes);
-  A(S.tA, nodes);
-  A(S.tB, nodes);
+  A(S.tN, nodes); // cudaMalloc: 256-byte aligned, so every record is 32
   A(S.tM, nodes);
   // scan / sort scratch
   SortScratch &so = h->sort;

@@ -499,12 +499,13 @@ __global__ void __launch_bounds__(kBlock) k_preorder(DevState S) {
     if (S.subtree[g] == 0 || pre >= G.nodeCount) continue; // empty node
     const uint32_t pg = nb + pre;
     const float sz = S.size[g];
-    S.tA[pg] = make_float4(S.comX[g], S.comY[g], S.mass[g], __fmul_rn(sz, sz));
+    TravNode &T = S.tN[pg];
+    T.a = make_float4(S.comX[g], S.comY[g], S.mass[g], __fmul_rn(sz, sz));
     // next node after this subtree; all ones past the instance's last node
     const uint32_t skip = pg + S.subtree[g];
     const uint32_t nextPg = skip >= nb + S.subtree[nb] ? 0xffffffffu : skip;
-    S.tB[pg] = make_int4((int)nextPg, (int)(G.start + S.start[g]),
-                         (int)(G.start + S.end[g]), S.children[g] == 0 ? 1 : 0);
+    T.b = make_int4((int)nextPg, (int)(G.start + S.start[g]), (int)(G.start + S.end[g]),
+                    S.children[g] == 0 ? 1 : 0);
     const float4 mo = S.moments[g];
     S.tM[pg] = make_float4(mo.x, mo.y, mo.z, sz);
     S.tC[pg] = make_float2(S.centerX[g], S.centerY[g]);

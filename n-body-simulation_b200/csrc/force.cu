@@ -33,6 +33,15 @@ constexpr int kForceBlock = 256;
 constexpr int kWarps = kForceBlock / 32;
 constexpr uint32_t kDone = 0xffffffffu;
 
+// One traversal record with a single 256-bit read-only load (sm_100); the
+// records are 32-byte aligned (TravNode).
+__device__ __forceinline__ void ld_node(const TravNode *p, float4 &a, int4 &b) {
+  asm("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z),
+        "=r"(b.w)
+      : "l"(p));
+}
+
 __device__ __forceinline__ float rcp_approx(float x) {
   float r;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
@@ -132,9 +141,10 @@ __device__ __forceinline__ void walk_targets(
     const uint32_t k = __reduce_min_sync(0xffffffffu, cur);
     if (k == kDone) break;
     if (kCount) ++nIter;
-    // k is the same for the whole warp: one broadcast load through L1
-    const float4 A = __ldg(&S.tA[k]);
-    const int4 B = __ldg(&S.tB[k]);
+    // k is the same for the whole warp: one broadcast 256-bit load
+    float4 A;
+    int4 B;
+    ld_node(&S.tN[k], A, B);
     // the node after k's subtree (kDone past the instance's last node)
     const uint32_t nxt = (uint32_t)B.x;
     // every lane evaluates the node; only the lanes waiting at it use it

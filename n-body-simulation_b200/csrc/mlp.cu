@@ -41,8 +41,8 @@ __global__ void k_harvest_walk(DevState S, const uint32_t *__restrict__ targets,
     uint32_t cur = G.nodeBase, end = G.nodeBase + G.travCount;
     uint32_t guard = 0;
     while (cur < end && ++guard < (1u << 24)) {
-      const float4 A = S.tA[cur];
-      const int4 B = S.tB[cur];
+      const float4 A = S.tN[cur].a;
+      const int4 B = S.tN[cur].b;
       const float dx = A.x - P.x, dy = A.y - P.y;
       const float dSq = dx * dx + dy * dy;
       const uint32_t nxt = (uint32_t)B.x > cur ? (uint32_t)B.x : end;
@@ -73,8 +73,8 @@ __global__ void k_harvest_rows(DevState S, const uint2 *__restrict__ items,
     const uint2 pr = items[it];
     const uint32_t t = pr.x, g = pr.y;
     const float4 P = S.xym[t];
-    const float4 A = S.tA[g];
-    const int4 B = S.tB[g];
+    const float4 A = S.tN[g].a;
+    const int4 B = S.tN[g].b;
     const float4 M = S.tM[g];
     const float2 Q = S.tC[g];
     const double e2 = (double)eps * eps;

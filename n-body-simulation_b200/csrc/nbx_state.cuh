@@ -24,6 +24,16 @@ struct SegDev {
   uint32_t pad2[2];
 };
 
+// A node of the force traversal, in depth-first preorder: a = {comX, comY,
+// mass, size*size}, b = {next (preorder, global; all ones past the
+// instance's last node), start, end, isLeaf}.  32-byte aligned so that the
+// traversal reads a record with one 256-bit load.
+struct alignas(32) TravNode {
+  float4 a;
+  int4 b;
+};
+static_assert(sizeof(TravNode) == 32, "32-byte traversal records");
+
 constexpr int kMaxDepth = 32;   // TreeKernels.cuh:29
 constexpr int kLevelSlots = 34; // depths 0..32 plus an end slot
 
@@ -115,8 +125,7 @@ struct DevState {
   uint32_t *subtree;    // nodes in subtree
   uint32_t *arrive;     // bottom-up arrival counters
   // traversal layout (preorder)
-  float4 *tA; // {comX, comY, mass, size*size}
-  int4 *tB;   // {next (preorder, global), start, end, isLeaf}
+  TravNode *tN; // preorder traversal records (32 bytes, one load each)
   float4 *tM; // {Ixx, Iyy, Ixy, size} for the learned correction
   float2 *tC; // square centre, for the learned correction
 
