@@ -410,7 +410,7 @@ int allocate(nbx_handle *h) {
   A(so.vals[0], sortCap);
   A(so.vals[1], sortCap);
   A(so.hist, 8 * 256);
-  A(so.status, (size_t)so.maxTiles * 256 + 256);
+  A(so.status, 8 * ((size_t)so.maxTiles * 256 + 256));
   A(so.tileCounter, 8);
   ScanScratch &sc = h->scan;
   sc.maxTiles = (uint32_t)scan_scratch_tiles(std::max<uint32_t>(S.nBuckets + 2, sortCap));
@@ -1148,7 +1148,7 @@ int nbx_render(nbx_handle *h, const nbx_camera *cam, const nbx_draw *d, uint32_t
     if (!so.tileCounter) NBX_CUDA(h, cudaMalloc(&so.tileCounter, 8 * sizeof(uint32_t)));
     so.capacity = cap;
     so.maxTiles = (uint32_t)sort_tiles(cap);
-    NBX_CUDA(h, grow(so.status, (size_t)so.maxTiles * 256 + 256));
+    NBX_CUDA(h, grow(so.status, 8 * ((size_t)so.maxTiles * 256 + 256)));
     r.entries = cap;
   }
   int bits = 8;

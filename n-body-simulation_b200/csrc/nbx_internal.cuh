@@ -120,7 +120,7 @@ struct SortScratch {
   uint64_t *keys[2] = {nullptr, nullptr};
   uint32_t *vals[2] = {nullptr, nullptr};
   uint32_t *hist = nullptr;        // [8 passes][256] digit counts
-  uint32_t *status = nullptr;      // [maxTiles][256] look-back words
+  uint32_t *status = nullptr;      // [8 passes][maxTiles][256] look-back words
   uint32_t *tileCounter = nullptr; // [8]
   uint32_t maxTiles = 0;
   uint32_t capacity = 0;

@@ -526,19 +526,22 @@ int radix_sort_u64(cudaStream_t s, SortScratch &sc, uint32_t n_max,
   k_radix_hist_scan<<<np, 256, 0, s>>>(sc.hist, p0);
   const uint32_t tiles = (n_max + kSortTile - 1) / kSortTile;
   cudaMemsetAsync(sc.tileCounter, 0, sizeof(uint32_t) * 8, s);
+  // look-back words of every pass, cleared at once
+  const size_t passWords = 256 * (size_t)(tiles + 1);
+  cudaMemsetAsync(sc.status, 0, sizeof(uint32_t) * passWords * np, s);
   int cur = 0;
   for (int p = 0; p < np; ++p) {
-    cudaMemsetAsync(sc.status, 0, sizeof(uint32_t) * 256 * (tiles + 1), s);
+    uint32_t *status = sc.status + passWords * p;
     const int shift = 8 * (p0 + p);
     if (p == 0 && vals_identity) {
       k_onesweep<true><<<tiles > 0 ? tiles : 1, kSortThreads, 0, s>>>(
           sc.keys[cur], sc.vals[cur], sc.keys[cur ^ 1], sc.vals[cur ^ 1],
-          sc.hist + (p0 + p) * 256, sc.status, sc.tileCounter + p, n_max, d_n,
+          sc.hist + (p0 + p) * 256, status, sc.tileCounter + p, n_max, d_n,
           shift, err);
     } else {
       k_onesweep<false><<<tiles > 0 ? tiles : 1, kSortThreads, 0, s>>>(
           sc.keys[cur], sc.vals[cur], sc.keys[cur ^ 1], sc.vals[cur ^ 1],
-          sc.hist + (p0 + p) * 256, sc.status, sc.tileCounter + p, n_max, d_n,
+          sc.hist + (p0 + p) * 256, status, sc.tileCounter + p, n_max, d_n,
           shift, err);
     }
     cur ^= 1;
