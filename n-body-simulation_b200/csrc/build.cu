@@ -504,8 +504,12 @@ __global__ void __launch_bounds__(kBlock) k_preorder(DevState S) {
     // next node after this subtree; all ones past the instance's last node
     const uint32_t skip = pg + S.subtree[g];
     const uint32_t nextPg = skip >= nb + S.subtree[nb] ? 0xffffffffu : skip;
-    T.b = make_int4((int)nextPg, (int)(G.start + S.start[g]), (int)(G.start + S.end[g]),
-                    S.children[g] == 0 ? 1 : 0);
+    // where a lane that opens this node goes next: a leaf is summed and
+    // skipped, an interior node descends to its first child (the next
+    // preorder slot)
+    const uint32_t openPg = S.children[g] == 0 ? nextPg : pg + 1;
+    T.b = make_int4((int)nextPg, (int)openPg, (int)(G.start + S.start[g]),
+                    (int)(G.start + S.end[g]));
     const float4 mo = S.moments[g];
     S.tM[pg] = make_float4(mo.x, mo.y, mo.z, sz);
     S.tC[pg] = make_float2(S.centerX[g], S.centerY[g]);

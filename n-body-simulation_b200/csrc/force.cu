@@ -154,7 +154,7 @@ __device__ __forceinline__ void walk_targets(
     const float dSq = sq_dist<kExact>(dx, dy);
     const float far = kExact ? __fmul_rn(dSq, tSq) : dSq * tSq;
     const bool accept = at && A.w < far;
-    const bool openLeaf = at && !accept && B.w != 0;
+    const bool openLeaf = at && !accept && B.y == B.x; // leaf: open == next
     {
       const bool use = accept && A.z > 0.0f;
       const float fac = law_factor<kExact, kClamp>(dSq, A.z, eSq);
@@ -203,11 +203,12 @@ __device__ __forceinline__ void walk_targets(
       if (kCount) nFar += use ? 1u : 0u;
     }
     if (kCount) nVisit += at ? 1u : 0u;
-    // accepted or leaf: skip the subtree; interior node: descend
-    cur = (accept || openLeaf) ? nxt : (at ? k + 1 : cur);
+    // accepted: skip the subtree; opened: the node's open slot (skip a
+    // leaf, descend into an interior node)
+    cur = at ? (accept ? nxt : (uint32_t)B.y) : cur;
     const uint32_t leafLanes = __ballot_sync(0xffffffffu, openLeaf);
     if (leafLanes) {
-      const uint32_t b0 = (uint32_t)B.y, b1 = (uint32_t)B.z;
+      const uint32_t b0 = (uint32_t)B.z, b1 = (uint32_t)B.w;
       const uint32_t bEnd = b1 <= S.n ? b1 : S.n; // defensive bound
       for (uint32_t base = b0; base < bEnd; base += 32) {
         const uint32_t cnt = min(32u, bEnd - base);
@@ -305,9 +306,11 @@ __device__ __forceinline__ void forces_walk(
 // which the host picks only for non-negative masses below its bound; a
 // warp holding a target whose instance reaches beyond the coordinate limit
 // stored at upload (the build's SegDev::wide), where distances could
-// overflow, takes the clamped walk instead.
+// overflow, takes the clamped walk instead.  Launch bounds: 8 blocks of 256
+// threads per SM (at most 32 registers, none spilled) for every walk but the
+// learned correction's, whose MMA fragments keep it at 3.
 template <bool kExact, bool kCount = false, int kCorr = 0, bool kClamp = true>
-__global__ void __launch_bounds__(kForceBlock)
+__global__ void __launch_bounds__(kForceBlock, kCorr == 1 ? 3 : 8)
     k_forces(DevState S, float tSq, float eSq,
              unsigned long long *counts = nullptr,
              const MlpDev *__restrict__ mlp = nullptr, float bandSq = 0.0f,

@@ -52,7 +52,7 @@ __global__ void k_harvest_walk(DevState S, const uint32_t *__restrict__ targets,
           if (slot < cap) items[slot] = make_uint2(t, cur);
         }
         cur = nxt;
-      } else if (B.w) {
+      } else if (B.y == B.x) { // leaf
         cur = nxt;
       } else {
         cur = cur + 1;
@@ -79,7 +79,7 @@ __global__ void k_harvest_rows(DevState S, const uint2 *__restrict__ items,
     const float2 Q = S.tC[g];
     const double e2 = (double)eps * eps;
     double sx = 0.0, sy = 0.0;
-    for (int j = B.y + lane; j < B.z; j += 32) {
+    for (int j = B.z + lane; j < B.w; j += 32) {
       if ((uint32_t)j == t) continue;
       const float4 b = S.xym[j];
       const double dx = (double)b.x - P.x, dy = (double)b.y - P.y;

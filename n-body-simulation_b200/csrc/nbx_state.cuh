@@ -25,8 +25,11 @@ struct SegDev {
 };
 
 // A node of the force traversal, in depth-first preorder: a = {comX, comY,
-// mass, size*size}, b = {next (preorder, global; all ones past the
-// instance's last node), start, end, isLeaf}.  32-byte aligned so that the
+// mass, size*size}, b = {next, open, start, end}: next = the slot after the
+// node's subtree (preorder, global; all ones past the instance's last node),
+// open = where a walk that opens the node goes (next for a leaf, the next
+// slot -- its first child -- for an interior node, so a node is a leaf iff
+// open == next), [start, end) = its bodies.  32-byte aligned so that the
 // traversal reads a record with one 256-bit load.
 struct alignas(32) TravNode {
   float4 a;
