@@ -156,7 +156,11 @@ __device__ __forceinline__ void walk_targets(
     const bool accept = at && A.w < far;
     const bool openLeaf = at && !accept && B.y == B.x; // leaf: open == next
     {
-      const bool use = accept && A.z > 0.0f;
+      // the reference adds a cell only if its mass is > 0; in the clamp-free
+      // plain walk masses are >= 0 and every term is finite, so a massless
+      // cell's term is exactly +-0 and the mass test can go
+      constexpr bool kZeroMassAddsNothing = !kExact && !kClamp && kCorr == 0;
+      const bool use = accept && (kZeroMassAddsNothing || A.z > 0.0f);
       const float fac = law_factor<kExact, kClamp>(dSq, A.z, eSq);
       float tx, ty;
       if (kExact) {
