@@ -61,7 +61,7 @@ FLOP_PER_INTERACTION = 20.0
 ALG_BYTES_PER_BODY_STEP = 285.0 - 16.0  # the force pass's 16 B excluded
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_forces
 # launch on the two-disc 1M workload, from an ncu capture of its third launch.
-FORCE_TRAFFIC_BYTES = 23.706112e6
+FORCE_TRAFFIC_BYTES = 23.705856e6
 
 
 def parse():
