@@ -164,14 +164,20 @@ def barrier(dist):
         dist.barrier()
 
 
+def parallelism(world: int) -> str:
+    """Both arms name the same layout: one replica of the simulation per GPU."""
+    return f"replicas{world}" if world > 1 else "single"
+
+
 # ------------------------------------------------------------- reference
 def reference_rate(n, steps, warmup, bodies=None):
-    """The reference's OpenMP Simulation::step (its own flags), all cores."""
+    """The reference's OpenMP Simulation::step (its own flags), all cores.
+    Without `bodies` the workload is built by the reference's own
+    uniformDisc (oracle/_ref), so that this arm maps no product code."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import Reference
     R = Reference("omp")
-    import nbx
-    b = bodies if bodies is not None else nbx.two_discs(n, 0, 0.2)
+    b = bodies if bodies is not None else R.two_discs(n, 0, 0.2)
     if warmup:
         b, _ = R.simulate(b, theta=THETA, steps=warmup)
     _, ms = R.simulate(b, theta=THETA, steps=steps)
@@ -190,10 +196,11 @@ def run_reference(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": steps, "warmup": warm, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic", "config": WORKLOAD,
+        "dtype": "f32", "data": "synthetic",
+        "config": dict(WORKLOAD, parallelism=parallelism(args.gpus)),
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores,
-                         "kind": "reference",
+                         "kind": "reference", "host": host_cpu(),
                          "sample": f"{steps} Simulation::step calls of the "
                                    f"{args.n}-body workload after {warm} warm-up "
                                    "steps (requested steps capped at 20)"},
@@ -271,31 +278,172 @@ def render_leg(nbx, sim, n):
     return res
 
 
-def cold_square_leg(nbx, torch, local):
-    """The collision-heavy cold-square collapse at its full size: 4,194,304
-    unit masses at rest (the viewer's ColdSquare geometry, softening 1e-3 of
-    the half-width), theta 0.5, collisions on; 200 steps (the configuration
-    runs 2000); momentum and angular momentum from compensated FP64 sums."""
+def cold_square_leg(nbx, torch, local, steps=2000, every=100, samples=16384):
+    """The collision-heavy cold-square collapse at its full size and
+    configured length: 4,194,304 unit masses at rest (the viewer's
+    ColdSquare geometry, softening 1e-3 of the half-width), theta 0.5,
+    collisions on, 2000 steps through the densest-core phase.  Every `every`
+    steps: ms/step of the graph steps, one eagerly profiled step (the
+    ordered resolution's share of it), the contact pairs and the longest
+    chain of dependent pairs.  Energy drift: compensated FP64 kinetic energy
+    of all bodies plus the FP64 potential of the tree law estimated from
+    the same `samples` bodies (by id) at the start and the end."""
     n = 1 << 22
     eps = 1e-3 * 3.0 * float(np.sqrt(n))
     sim = nbx.Simulation(nbx.cold_square(n, 0), theta=0.5, epsilon=eps, device=local)
     stream = torch.cuda.ExternalStream(sim.stream(), device=local)
-    em0 = sim.energy_momentum()
-    sim.step(3)
+    rng = np.random.default_rng(777)
+    sample_ids = rng.choice(n, samples, replace=False)
+
+    def energy():
+        st = sim.download()
+        where = np.empty(n, np.int64)
+        where[st["id"]] = np.arange(n)
+        tg = where[sample_ids].astype(np.uint32)
+        u, phi = sim.potential(tg)
+        mphi = st["mass"][tg].astype(np.float64) * phi
+        u_err = 0.5 * n * float(np.std(mphi)) / np.sqrt(samples)
+        em = sim.energy_momentum()
+        mv = float(np.sum(st["mass"].astype(np.float64)
+                          * np.hypot(st["vx"].astype(np.float64), st["vy"].astype(np.float64))))
+        return em, u, u_err, mv
+
+    em0, u0, u0_err, _ = energy()
+    trace = []
+    total_ms = 0.0
+    done = 0
+    while done < steps:
+        k = min(every, steps - done)
+        ms = time_steps(torch, sim, stream, k - 1) if k > 1 else 0.0
+        prof = sim.profile_step()
+        pairs, depth = sim.collision_stats()
+        step_ms = sum(prof.values())
+        total_ms += ms * (k - 1) + step_ms
+        done += k
+        trace.append({"step": done, "ms_per_step": ms if k > 1 else step_ms,
+                      "resolve_share": prof.get("collide.resolve", 0.0) / step_ms,
+                      "contact_pairs": pairs, "chain_depth": depth})
     sim.sync()
-    steps = 200
-    ms = time_steps(torch, sim, stream, steps)
-    em = sim.energy_momentum()
-    s = sim.download()
-    mv = float(np.sum(s["mass"].astype(np.float64)
-                      * np.hypot(s["vx"].astype(np.float64), s["vy"].astype(np.float64))))
+    em, u, u_err, mv = energy()
     sim.close()
-    return {"bodies": n, "steps": steps, "epsilon": eps, "ms_per_step": ms,
-            "body_steps_per_s": n / (ms * 1e-3),
-            "kinetic_energy_fp64": float(em[0]),
+    e0 = em0[0] + u0
+    e1 = em[0] + u
+    return {"bodies": n, "steps": steps, "epsilon": eps, "theta": 0.5,
+            "ms_per_step": total_ms / steps,
+            "body_steps_per_s": n * steps / (total_ms * 1e-3),
+            "per_100_steps": trace,
+            "kinetic_energy_fp64": [float(em0[0]), float(em[0])],
+            "potential_energy_fp64": [u0, u],
+            "potential_sample_stderr": [u0_err, u_err],
+            "energy_drift_rel": (e1 - e0) / abs(e0),
+            "energy_drift_rel_stderr": float(np.hypot(u0_err, u_err)) / abs(e0),
+            "energy_note": "potential from the FP64 tree-law direct sum at the "
+                           f"same {samples} bodies (by id) at both ends, scaled "
+                           "to all pairs; collisions are inelastic, so total "
+                           "energy falls physically",
             "momentum_drift_rel": float(np.hypot(em[1] - em0[1], em[2] - em0[2])) / mv,
             "angular_momentum_drift_rel": float(abs(em[3] - em0[3])) / (mv * 3.0 * np.sqrt(n)),
             "mass_exact": bool(em[4] == em0[4])}
+
+
+def host_cpu():
+    """Model name and logical CPU count of this host (lscpu's figures)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "nproc": os.cpu_count()}
+
+
+def _ref_gpu_child(n, kind, theta, warmup, steps, q):
+    """Child process: the reference's CudaSimulation (oracle/_ref/
+    libref_cuda.so) on its own CUDA context; the reference exits on any CUDA
+    error, which the parent then sees as a dead child."""
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from oracle import Reference, ReferenceCuda
+        R = Reference("omp")
+        b = R.two_discs(n, 0, 0.2) if kind == "two_discs" else R.uniform_disc(n, 0)
+        _, ms = ReferenceCuda().simulate(b, theta=theta, warmup=warmup, steps=steps)
+        q.put({"ms": ms})
+    except Exception as ex:  # reference build absent
+        q.put({"unavailable": str(ex)})
+
+
+def reference_gpu(n, kind, theta, warmup, steps):
+    """ms/step of the reference's own CUDA path (CudaSimulation::step,
+    built for sm_100a from its unmodified sources) on the same GPU, run in a
+    child process; its collisions are resolved Jacobi-style, every contact
+    of a body against the step's start state, by design
+    (accumulatePair, CollisionKernels.cuh:197-235)."""
+    import multiprocessing as mpc
+    ctx = mpc.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_ref_gpu_child, args=(n, kind, theta, warmup, steps, q))
+    p.start()
+    p.join(600)
+    if p.is_alive():
+        p.kill()
+        return {"unavailable": "timed out"}
+    if p.exitcode != 0 or q.empty():
+        return {"unavailable": f"reference exited with code {p.exitcode}"}
+    r = q.get()
+    if "ms" in r:
+        if r["ms"] < 0:
+            return {"unavailable": "CUDA error in the reference path"}
+        ms = r["ms"] / steps
+        return {"ms_per_step": ms, "body_steps_per_s": n / (ms * 1e-3),
+                "steps": steps, "warmup": warmup}
+    return r
+
+
+def c0_leg(nbx, torch, local):
+    """The reference's own CPU-runnable case: uniformDisc(10,000), dt 0.05,
+    eps 1, leaf 16, collisions on, 100 steps, at theta 1.0 (the reference's
+    default, what its `sim` CLI runs) and 0.5.  The product (device-resident
+    step graphs, CUDA events) against the reference's serial and OpenMP
+    builds (its own flags; the CLIs' avg_compute_step at theta 1.0 as well)
+    and its CUDA path on the same GPU."""
+    n, steps = 10000, 100
+    res = {"bodies": n, "steps": steps, "host": host_cpu()}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    for theta in (1.0, 0.5):
+        row = {}
+        sim = nbx.Simulation(nbx.uniform_disc(n), theta=theta, device=local)
+        stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+        sim.step(3)
+        ms = time_steps(torch, sim, stream, steps)
+        sim.close()
+        row["b200"] = {"ms_per_step": ms, "body_steps_per_s": n / (ms * 1e-3)}
+        try:
+            from oracle import Reference
+            for kind in ("serial", "omp"):
+                R = Reference(kind)
+                _, rms = R.simulate(nbx.uniform_disc(n), theta=theta, steps=steps)
+                row[f"reference_{kind}"] = {"ms_per_step": rms / steps,
+                                            "body_steps_per_s": n * steps / (rms * 1e-3),
+                                            "threads": R.threads()}
+        except Exception as ex:
+            row["reference_cpu"] = {"unavailable": str(ex)}
+        row["reference_cuda"] = reference_gpu(n, "disc", theta, 3, steps)
+        res[f"theta_{theta}"] = row
+    # the reference CLIs themselves (theta 1.0), their own timing line
+    for exe in ("sim_serial", "sim"):
+        path = os.path.join(ROOT, "oracle", "_ref", exe)
+        try:
+            out = subprocess.run([path, str(n), str(steps), "1"], capture_output=True,
+                                 text=True, timeout=300).stderr
+            avg = float(out.split("avg_compute_step=")[1].split()[0])
+            res[f"cli_{exe}"] = {"avg_compute_step_ms": avg,
+                                 "body_steps_per_s": n / (avg * 1e-3)}
+        except (OSError, IndexError, ValueError, subprocess.SubprocessError) as ex:
+            res[f"cli_{exe}"] = {"unavailable": str(ex)}
+    return res
 
 
 NAIVE_N = 1 << 18
@@ -364,12 +512,18 @@ def ensemble_leg(nbx, torch, world, rank, local, dist, args):
     h.step(2)
     kernels = h.step_kernels()
     ms = max_over_ranks(dist, local, time_steps(torch, h, stream, steps))
-    h.close()
     total = int(sizes.sum())
     res = {"instances": int(len(sizes)), "bodies": total, "theta": 0.5,
            "steps": steps, "ms_per_step": ms,
            "body_steps_per_s": total / (ms * 1e-3),
            "kernels_per_step": kernels}
+    if dist is not None:
+        # the run's only collective: per-instance metrics to every rank
+        metrics = ensemble.gather_metrics(
+            dist, mine, ensemble.instance_metrics(h.download(), my_sizes),
+            len(sizes), local)
+        res["gathered_instances"] = int(np.isfinite(metrics[:, 0]).sum())
+    h.close()
     if world == 1:
         loop_steps = 3
         hs = []
@@ -514,12 +668,19 @@ def run_b200(args):
     naive = naive_leg(nbx, torch, local, args) if not args.quick else None
     cold = cold_square_leg(nbx, torch, local) if not args.quick else None
     render = render_leg(nbx, sim_keep, n) if not args.quick else None
+    c0 = ref_gpu = None
+    if rank == 0 and world == 1 and not args.quick and not args.no_cpu_baseline:
+        c0 = c0_leg(nbx, torch, local)
+        # the reference's own CUDA path on the same GPU, headline workload
+        ref_gpu = dict(reference_gpu(n, "two_discs", THETA, 3, min(max(args.steps, 5), 20)),
+                       workload=WORKLOAD["workload"])
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             v, cores, cms = reference_rate(n, 8, 1, bodies)
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                   "host": host_cpu(),
                    "sample": f"8 Simulation::step calls of the same {n}-body "
                              f"workload after 1 warm-up step ({cms:.0f} ms/step), "
                              "reference built with its own flags (-Ofast -fopenmp)"}
@@ -533,7 +694,7 @@ def run_b200(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": dict(WORKLOAD, parallelism=f"replicas{world}" if world > 1 else "single"),
+        "config": dict(WORKLOAD, parallelism=parallelism(world)),
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": 36 * n, "d2h_bytes_per_step": 36 * n,
                 "ms_per_step": e2e_ms},
@@ -581,6 +742,10 @@ def run_b200(args):
         line["cold_square"] = cold
     if render is not None:
         line["render"] = render
+    if c0 is not None:
+        line["c0_disc10k"] = c0
+    if ref_gpu is not None:
+        line["reference_gpu_baseline"] = ref_gpu
     if cpu is not None:
         line["cpu_baseline"] = cpu
     if rank == 0:

@@ -215,6 +215,13 @@ int nbx_get_tree(nbx_handle *h, uint32_t instance, float *com_x, float *com_y,
 int nbx_get_pairs(nbx_handle *h, int32_t *later, int32_t *earlier,
                   int64_t capacity, int64_t *count);
 
+/* Contact statistics of the last collide: *pairs the candidate pairs it
+ * resolved, *depth the longest chain of pairs that each wait for an
+ * earlier pair sharing a body (the length of the sequential dependence in
+ * Collision.cpp:341-348, which bounds the ordered resolution's time).  No
+ * counterpart in the reference. */
+int nbx_collision_stats(nbx_handle *h, int64_t *pairs, uint32_t *depth);
+
 /* Accelerations at arbitrary points (px[i], py[i]) from instance 0's last
  * tree, with the handle's theta/epsilon: QuadTree::acceleration(pos, bodies)
  * for any position (QuadTree.h:83-85, QuadTree.cpp:264-389). */
@@ -274,14 +281,20 @@ int nbx_direct_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m,
  * must not pay cudaMalloc's device-wide synchronisation inside a loop).  No
  * counterpart in the reference.  Every pointer is DEVICE memory owned by
  * the caller: body positions x, y and masses (n floats each, the bodies'
- * current order), targets (m indices), outputs ax, ay (m doubles); runs on
- * `stream` (cudaStream_t, NULL = default stream) on the current device.
+ * current order), targets (m indices, each in 0..n-1; a target outside
+ * that range is not read through and gets NaN outputs), outputs ax, ay
+ * (m doubles); runs on `stream` (cudaStream_t, NULL = default stream) on
+ * the current device.  It sums the tree law m d / (|d| (d^2 + eps^2)) over
+ * all n bodies given, as nbx_direct_fp64 does for a single-instance handle
+ * with force_law 0 (no Plummer law, no per-instance source ranges).
  * Allocates nothing: its partial sums live in a fixed 4 MiB device array of
  * the library, held by every GPU that loads it until exit.  At most 4096
  * targets per call (NBX_ERR_CAPACITY beyond).  The first call on a device
- * looks up that array's address; make it before any stream capture.  Calls
- * share the array: calls whose kernels overlap on the GPU race, so order
- * them on one stream. */
+ * looks up that array's address and keeps it; make it before any stream
+ * capture, and do not call it again on a device after cudaDeviceReset.
+ * Calls share the array: calls whose kernels overlap on the GPU race, so
+ * order them on one stream.  Launch failures are those of its own launches;
+ * an error left pending by earlier CUDA calls is not cleared. */
 int nbx_direct_fp64_noalloc(const float *x, const float *y, const float *mass,
                             uint32_t n, const uint32_t *targets, uint32_t m,
                             double epsilon, double *ax, double *ay,
@@ -296,6 +309,21 @@ int nbx_force_error_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m,
 /* Compensated FP64 sums over all bodies: {kinetic energy, px, py, Lz,
  * total mass}.  No counterpart in the reference. */
 int nbx_energy_momentum_fp64(nbx_handle *h, double *out5);
+
+/* FP64 potential energy of the handle's force law, the partner of
+ * nbx_energy_momentum_fp64's kinetic energy for total-energy drift.  The
+ * pair potential is the one whose gradient is the law: for the tree law
+ * m d / (|d| (d^2 + eps^2)) (exactTreeLawForces, CheckCuda.cu:453-475) it
+ * is -m_i m_j atan(eps / r) / eps (-m_i m_j / r for eps = 0); for
+ * force_law 1, -m_i m_j / sqrt(r^2 + eps^2).  Pairs are taken within each
+ * instance.  targets == NULL: *u = the exact sum over all pairs (every body
+ * a target of an FP64 direct sum, O(n^2): for test sizes or occasional
+ * checks; compensated over the targets).  Otherwise phi[k] receives the
+ * potential per unit mass at body targets[k] (current index) from every
+ * other body of its instance, and *u the sampled estimate
+ * (n / m) * 1/2 * sum_k mass_k * phi[k].  No counterpart in the reference. */
+int nbx_potential_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m,
+                       double *phi, double *u);
 
 /* --- measurement helpers (no counterpart in the reference) --- */
 

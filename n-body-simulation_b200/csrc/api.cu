@@ -1422,13 +1422,37 @@ int nbx_get_pairs(nbx_handle *h, int32_t *later, int32_t *earlier, int64_t cap,
   return NBX_OK;
 }
 
-int nbx_direct_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m, double *ax,
-                    double *ay) {
-  if (!h || (m && (!targets || !ax || !ay))) return NBX_ERR_ARG;
-  cudaSetDevice(h->device);
-  if (m == 0) return NBX_OK;
-  for (uint32_t k = 0; k < m; ++k)
-    if (targets[k] >= h->n) return fail(h, NBX_ERR_ARG, "target index out of range");
+int nbx_collision_stats(nbx_handle *h, int64_t *pairs, uint32_t *depth) {
+  if (!h || !pairs || !depth) return NBX_ERR_ARG;
+  int64_t total = 0;
+  int rc = nbx_get_pairs(h, nullptr, nullptr, 0, &total);
+  if (rc) return rc;
+  std::vector<int32_t> later((size_t)total), earlier((size_t)total);
+  rc = nbx_get_pairs(h, later.data(), earlier.data(), total, &total);
+  if (rc) return rc;
+  // a pair waits for the last earlier pair of either body (the sequential
+  // loop's order, Collision.cpp:341-348): longest chain of such waits
+  std::vector<uint32_t> last(h->n, 0u);
+  uint32_t deepest = 0;
+  for (int64_t k = 0; k < total; ++k) {
+    const uint32_t a = (uint32_t)later[k], b = (uint32_t)earlier[k];
+    const uint32_t d = std::max(last[a], last[b]) + 1u;
+    last[a] = last[b] = d;
+    deepest = std::max(deepest, d);
+  }
+  *pairs = total;
+  *depth = deepest;
+  return NBX_OK;
+}
+
+} // extern "C"
+
+namespace {
+// FP64 direct sums for targets at the given current indices (checked by
+// the caller) over the bodies of each target's own instance; kind as
+// launch_direct_fp64.  Writes m values to ax (and to ay for forces).
+int direct_sums(nbx_handle *h, const uint32_t *targets, uint32_t m, int kind,
+                double *ax, double *ay) {
   if (h->dPartialTargets < m) {
     if (h->dPartial) cudaFree(h->dPartial);
     if (h->dTargets) cudaFree(h->dTargets);
@@ -1455,12 +1479,77 @@ int nbx_direct_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m, double *
   NBX_CUDA(h, cudaMemcpyAsync(dRanges, staged.data() + m, 8ull * m, cudaMemcpyHostToDevice, h->stream));
   const DevState S = h->state();
   launch_direct_fp64(h->stream, S.pv, S.mr, h->n, h->dTargets, dRanges, m,
-                     h->params.epsilon, h->params.force_law == 1 ? 1 : 0, h->dPartial,
-                     dOut, dOut + m);
+                     h->params.epsilon, kind, h->dPartial, dOut, dOut + m);
   NBX_CUDA(h, cudaGetLastError());
   NBX_CUDA(h, cudaMemcpyAsync(ax, dOut, 8ull * m, cudaMemcpyDeviceToHost, h->stream));
-  NBX_CUDA(h, cudaMemcpyAsync(ay, dOut + m, 8ull * m, cudaMemcpyDeviceToHost, h->stream));
+  if (ay)
+    NBX_CUDA(h, cudaMemcpyAsync(ay, dOut + m, 8ull * m, cudaMemcpyDeviceToHost, h->stream));
   NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  return NBX_OK;
+}
+
+// Neumaier accumulation in FP64 (host side of the compensated sums).
+struct HostKSum {
+  double s = 0.0, c = 0.0;
+  void add(double v) {
+    const double t = s + v;
+    if (std::fabs(s) >= std::fabs(v)) c += (s - t) + v;
+    else c += (v - t) + s;
+    s = t;
+  }
+  double value() const { return s + c; }
+};
+} // namespace
+
+extern "C" {
+
+int nbx_direct_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m, double *ax,
+                    double *ay) {
+  if (!h || (m && (!targets || !ax || !ay))) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (m == 0) return NBX_OK;
+  for (uint32_t k = 0; k < m; ++k)
+    if (targets[k] >= h->n) return fail(h, NBX_ERR_ARG, "target index out of range");
+  return direct_sums(h, targets, m, h->params.force_law == 1 ? 1 : 0, ax, ay);
+}
+
+int nbx_potential_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m, double *phi,
+                       double *u) {
+  if (!h || !u || (targets && m && !phi)) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  const int kind = h->params.force_law == 1 ? 3 : 2;
+  const DevState S = h->state();
+  if (targets) {
+    *u = 0.0;
+    if (m == 0) return NBX_OK;
+    for (uint32_t k = 0; k < m; ++k)
+      if (targets[k] >= h->n) return fail(h, NBX_ERR_ARG, "target index out of range");
+    int rc = direct_sums(h, targets, m, kind, phi, nullptr);
+    if (rc) return rc;
+    std::vector<float2> mr(h->n);
+    NBX_CUDA(h, cudaMemcpyAsync(mr.data(), S.mr, 8ull * h->n, cudaMemcpyDeviceToHost, h->stream));
+    NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+    HostKSum sum;
+    for (uint32_t k = 0; k < m; ++k) sum.add((double)mr[targets[k]].x * phi[k]);
+    *u = 0.5 * sum.value() * ((double)h->n / (double)m);
+    return NBX_OK;
+  }
+  // every body a target, in batches that keep the partial sums small
+  std::vector<float2> mr(h->n);
+  NBX_CUDA(h, cudaMemcpyAsync(mr.data(), S.mr, 8ull * h->n, cudaMemcpyDeviceToHost, h->stream));
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  constexpr uint32_t kBatch = 1u << 16;
+  std::vector<uint32_t> idx(std::min<size_t>(kBatch, h->n));
+  std::vector<double> ph(idx.size());
+  HostKSum sum;
+  for (uint32_t b0 = 0; b0 < h->n; b0 += kBatch) {
+    const uint32_t cnt = std::min<uint32_t>(kBatch, h->n - b0);
+    for (uint32_t k = 0; k < cnt; ++k) idx[k] = b0 + k;
+    int rc = direct_sums(h, idx.data(), cnt, kind, ph.data(), nullptr);
+    if (rc) return rc;
+    for (uint32_t k = 0; k < cnt; ++k) sum.add((double)mr[b0 + k].x * ph[k]);
+  }
+  *u = 0.5 * sum.value();
   return NBX_OK;
 }
 

@@ -10,13 +10,23 @@ namespace {
 constexpr int kDirectThreads = 128;
 constexpr int kDirectChunks = 64;
 
+// What a direct sum adds per source: the force of the tree law
+// m d / (|d| (d^2 + eps^2)) or of the Plummer law m d / (d^2 + eps^2)^1.5,
+// or the potential of either (per unit target mass): the tree law's is
+// -(m / eps) atan(eps / |d|) (its gradient is the tree force; -m / |d| for
+// eps = 0), the Plummer law's -m / sqrt(d^2 + eps^2).
+enum DirectKind { kTreeForce = 0, kPlummerForce = 1, kTreePotential = 2,
+                  kPlummerPotential = 3 };
+
 // Partial FP64 sums: block (tb, chunk) adds sources of `chunk` for the
 // targets tb*128 .. tb*128+127.  Sources staged through shared memory.
+// Potentials go to .x (.y stays 0).
 __global__ void __launch_bounds__(kDirectThreads)
     k_direct_partial(const float4 *__restrict__ pv, const float2 *__restrict__ mr,
                      uint32_t n, const uint32_t *__restrict__ targets,
                      const uint2 *__restrict__ ranges, uint32_t m, double eSq,
-                     int plummer, double2 *__restrict__ partial) {
+                     int kind, double2 *__restrict__ partial) {
+  const double eps = sqrt(eSq);
   __shared__ float4 sSrc[kDirectThreads];
   const uint32_t t = blockIdx.x * kDirectThreads + threadIdx.x;
   const bool valid = t < m;
@@ -51,12 +61,18 @@ __global__ void __launch_bounds__(kDirectThreads)
         const double dy = (double)s.y - y;
         const double dSq = dx * dx + dy * dy;
         if (dSq == 0.0) continue;
-        // tree law m d / (|d| (d^2 + eps^2)); Plummer m d / (d^2 + eps^2)^1.5
         const double q = dSq + eSq;
-        const double f = plummer ? (double)s.z / (q * sqrt(q))
-                                 : (double)s.z / (sqrt(dSq) * q);
-        ax += dx * f;
-        ay += dy * f;
+        if (kind == kTreeForce || kind == kPlummerForce) {
+          const double f = kind == kPlummerForce ? (double)s.z / (q * sqrt(q))
+                                                 : (double)s.z / (sqrt(dSq) * q);
+          ax += dx * f;
+          ay += dy * f;
+        } else if (kind == kPlummerPotential) {
+          ax -= (double)s.z / sqrt(q);
+        } else {
+          const double r = sqrt(dSq);
+          ax -= eps > 0.0 ? (double)s.z / eps * atan2(eps, r) : (double)s.z / r;
+        }
       }
     }
   }
@@ -138,14 +154,16 @@ __global__ void k_energy_final(const double *__restrict__ part, int blocks,
 } // namespace
 
 // partial must hold kDirectChunks * m double2.
+// kind: 0 tree-law force, 1 Plummer force, 2 tree-law potential (to ax),
+// 3 Plummer potential (to ax).
 void launch_direct_fp64(cudaStream_t s, const float4 *pv, const float2 *mr,
                         uint32_t n, const uint32_t *targets, const uint2 *ranges,
-                        uint32_t m, double eps, int plummer, double2 *partial,
+                        uint32_t m, double eps, int kind, double2 *partial,
                         double *ax, double *ay) {
   if (m == 0) return;
   dim3 grid((m + kDirectThreads - 1) / kDirectThreads, kDirectChunks);
   k_direct_partial<<<grid, kDirectThreads, 0, s>>>(pv, mr, n, targets, ranges, m,
-                                                   eps * eps, plummer, partial);
+                                                   eps * eps, kind, partial);
   k_direct_reduce<<<(m + 255) / 256, 256, 0, s>>>(partial, m, kDirectChunks, ax,
                                                   ay);
 }

@@ -26,7 +26,18 @@
 //    calls whose kernels overlap on the GPU (different streams, or
 //    different host threads) race on it: order them on one stream;
 //  * more than kNoallocMaxTargets targets is rejected with NBX_ERR_CAPACITY
-//    before anything is launched.
+//    before anything is launched;
+//  * a target index outside 0..n-1 is never read through: its outputs are
+//    NaN (the targets live in device memory, so the host cannot check them);
+//  * it sums the tree law m d / (|d| (d^2 + eps^2)) over all n bodies it is
+//    given (one contiguous body set), like nbx_direct_fp64 on a
+//    single-instance handle with force_law 0; it has no Plummer law and no
+//    per-instance source ranges;
+//  * the cached address does not survive cudaDeviceReset: a process that
+//    resets a device must not call it on that device again;
+//  * launch failures are taken from the launch calls themselves, so an
+//    error left pending by the caller's earlier CUDA calls is neither
+//    reported as this call's nor cleared.
 #include "nbx.h"
 
 #include <cuda_runtime.h>
@@ -53,8 +64,11 @@ __global__ void __launch_bounds__(kThreads)
                       double eSq, double2 *__restrict__ partial) {
   __shared__ float4 src[kThreads];
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
-  const bool valid = t < nt;
-  const uint32_t ti = valid ? targets[t] : 0u;
+  const uint32_t ti = t < nt ? targets[t] : 0u;
+  // an index outside the body array is not read through (its sums are
+  // replaced by NaN below)
+  const bool inRange = ti < n;
+  const bool valid = t < nt && inRange;
   const double px = valid ? (double)x[ti] : 0.0;
   const double py = valid ? (double)y[ti] : 0.0;
   const uint32_t chunk = (n + gridDim.y - 1) / gridDim.y;
@@ -81,7 +95,11 @@ __global__ void __launch_bounds__(kThreads)
       }
     }
   }
-  if (valid) partial[(size_t)blockIdx.y * nt + t] = make_double2(ax, ay);
+  if (t < nt) {
+    const double bad = __longlong_as_double(0x7ff8000000000000ll); // quiet NaN
+    partial[(size_t)blockIdx.y * nt + t] =
+        inRange ? make_double2(ax, ay) : make_double2(bad, bad);
+  }
 }
 
 __global__ void k_noalloc_reduce(const double2 *__restrict__ partial, uint32_t nt,
@@ -133,9 +151,20 @@ extern "C" int nbx_direct_fp64_noalloc(const float *x, const float *y,
   const int rc = partial_address(device, &partial);
   if (rc != NBX_OK) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const dim3 grid((m + kThreads - 1) / kThreads, kNoallocChunks);
-  k_noalloc_partial<<<grid, kThreads, 0, s>>>(x, y, mass, n, targets, m,
-                                              epsilon * epsilon, partial);
-  k_noalloc_reduce<<<(m + 255) / 256, 256, 0, s>>>(partial, m, ax, ay);
-  return cudaGetLastError() == cudaSuccess ? NBX_OK : NBX_ERR_CUDA;
+  // each launch's own return code: an error the caller left pending is not
+  // this call's to report or to clear
+  double eSq = epsilon * epsilon;
+  void *argsPartial[] = {(void *)&x, (void *)&y, (void *)&mass, (void *)&n,
+                         (void *)&targets, (void *)&m, (void *)&eSq,
+                         (void *)&partial};
+  if (cudaLaunchKernel((const void *)k_noalloc_partial,
+                       dim3((m + kThreads - 1) / kThreads, kNoallocChunks),
+                       dim3(kThreads), argsPartial, 0, s) != cudaSuccess)
+    return NBX_ERR_CUDA;
+  const double2 *part = partial;
+  void *argsReduce[] = {(void *)&part, (void *)&m, (void *)&ax, (void *)&ay};
+  if (cudaLaunchKernel((const void *)k_noalloc_reduce, dim3((m + 255) / 256),
+                       dim3(256), argsReduce, 0, s) != cudaSuccess)
+    return NBX_ERR_CUDA;
+  return NBX_OK;
 }

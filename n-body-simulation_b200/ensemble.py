@@ -41,20 +41,38 @@ def instance_metrics(bodies, sizes) -> np.ndarray:
     return out
 
 
-def gather_metrics(dist, local_ids, local_metrics, n_instances: int):
+def collective_device(backend: str, local_rank: int):
+    """Where a collective's buffers must live: NCCL moves only CUDA tensors
+    (on the rank's own device), gloo only host tensors."""
+    import torch
+    if str(backend).lower() == "nccl":
+        return torch.device("cuda", local_rank)
+    return torch.device("cpu")
+
+
+def gather_metrics(dist, local_ids, local_metrics, n_instances: int,
+                   local_rank: int | None = None):
     """All-gather of per-instance metrics to every rank (the run's only
-    collective).  `dist` is torch.distributed (gloo on CPU, nccl on GPU)."""
+    collective).  `dist` is torch.distributed (gloo on CPU, nccl on GPU);
+    the buffers are put where the group's backend needs them (for NCCL the
+    rank's CUDA device: `local_rank`, default the current device)."""
     import torch
     world = dist.get_world_size()
-    buf = torch.full((n_instances, local_metrics.shape[1] + 1), float("nan"),
-                     dtype=torch.float64)
+    backend = dist.get_backend()
+    if local_rank is None:
+        local_rank = torch.cuda.current_device() if str(backend).lower() == "nccl" else 0
+    dev = collective_device(backend, local_rank)
+    host = torch.full((n_instances, local_metrics.shape[1] + 1), float("nan"),
+                      dtype=torch.float64)
     for k, i in enumerate(local_ids):
-        buf[i, 0] = float(i)
-        buf[i, 1:] = torch.from_numpy(np.asarray(local_metrics[k], np.float64))
+        host[i, 0] = float(i)
+        host[i, 1:] = torch.from_numpy(np.asarray(local_metrics[k], np.float64))
+    buf = host.to(dev)
     parts = [torch.zeros_like(buf) for _ in range(world)]
     dist.all_gather(parts, buf)
-    full = torch.full_like(buf, float("nan"))
+    full = torch.full_like(host, float("nan"))
     for p in parts:
+        p = p.cpu()
         have = ~torch.isnan(p[:, 0])
         full[have] = p[have]
     return full[:, 1:].numpy()

@@ -41,6 +41,7 @@ EXPORTS = (
     "nbx_set_attractor", "nbx_reset", "nbx_nbs2_record", "nbx_nbs2_flush",
     "nbx_nbs2_open", "nbx_nbs2_write_packed", "nbx_nbs2_close",
     "nbx_draw_default", "nbx_render", "nbx_body_stats", "nbx_debug_expire_wait",
+    "nbx_potential_fp64", "nbx_collision_stats",
 )
 SCENARIOS = {"disc": 0, "two_galaxies": 1, "cold_square": 2}
 MLP_PARAMS = 1442
@@ -128,6 +129,8 @@ def lib() -> C.CDLL:
         "nbx_direct_fp64": [vp, u32p, C.c_uint32, f64p, f64p],
         "nbx_force_error_fp64": [vp, u32p, C.c_uint32, f64p, vp],
         "nbx_energy_momentum_fp64": [vp, f64p],
+        "nbx_potential_fp64": [vp, vp, C.c_uint32, vp, C.POINTER(C.c_double)],
+        "nbx_collision_stats": [vp, C.POINTER(C.c_int64), C.POINTER(C.c_uint32)],
         "nbx_status_bits": [vp, C.POINTER(C.c_uint32)],
         "nbx_last_error": [vp],
         "nbx_uniform_disc": [C.c_uint32, C.c_uint32, bodyp],
@@ -434,6 +437,13 @@ class Handle:
         self._c(lib().nbx_get_pairs(self.h, later, earlier, k, C.byref(cnt)))
         return later[:k], earlier[:k]
 
+    def collision_stats(self):
+        """(pairs, longest chain of dependent pairs) of the last collide."""
+        p = C.c_int64()
+        d = C.c_uint32()
+        self._c(lib().nbx_collision_stats(self.h, C.byref(p), C.byref(d)))
+        return p.value, d.value
+
     def direct_fp64(self, targets):
         t = np.ascontiguousarray(targets, np.uint32)
         ax = np.zeros(len(t), np.float64)
@@ -454,6 +464,19 @@ class Handle:
         out = np.zeros(5, np.float64)
         self._c(lib().nbx_energy_momentum_fp64(self.h, out))
         return out
+
+    def potential(self, targets=None):
+        """FP64 potential energy: exact over all pairs (targets None), or
+        (estimate, per-target potential per unit mass) for a sample."""
+        u = C.c_double()
+        if targets is None:
+            self._c(lib().nbx_potential_fp64(self.h, None, 0, None, C.byref(u)))
+            return u.value
+        t = np.ascontiguousarray(targets, np.uint32)
+        phi = np.zeros(len(t), np.float64)
+        self._c(lib().nbx_potential_fp64(self.h, t.ctypes.data, len(t),
+                                         phi.ctypes.data, C.byref(u)))
+        return u.value, phi
 
     def stream(self) -> int:
         s = C.c_void_p()

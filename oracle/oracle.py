@@ -286,8 +286,33 @@ class Oracle:
         return self.L.orc_potential_fp64(len(b), np.ascontiguousarray(b), eps)
 
 
+class ReferenceCuda:
+    """The reference's own CUDA path (oracle/_ref/libref_cuda.so:
+    CudaSimulation built for sm_100a from its unmodified sources).  The
+    reference exits the process on any CUDA error, so run it in a child
+    process."""
+
+    def __init__(self):
+        path = os.path.join(HERE, "_ref", "libref_cuda.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.L = C.CDLL(path)
+        self.L.ref_cuda_simulate.argtypes = [C.c_size_t, _bodyp, C.c_float, C.c_float,
+                                             C.c_float, C.c_int, C.c_int, C.c_int]
+        self.L.ref_cuda_simulate.restype = C.c_double
+
+    def simulate(self, b, dt=0.05, theta=1.0, eps=1.0, collisions=True, warmup=0,
+                 steps=1):
+        """(final state, ms of the timed steps)."""
+        b = np.ascontiguousarray(b.copy())
+        ms = self.L.ref_cuda_simulate(len(b), b, dt, theta, eps, int(collisions),
+                                      warmup, steps)
+        return b, ms
+
+
 class Reference:
-    """The reference's own code (oracle/_ref), serial IEEE or OpenMP build."""
+    """The reference's own code (oracle/_ref): serial IEEE ("parity"), its
+    own -Ofast OpenMP ("omp") or -Ofast serial ("serial") build."""
 
     def __init__(self, kind: str = "parity"):
         path = os.path.join(HERE, "_ref", f"libref_{kind}.so")
@@ -299,6 +324,7 @@ class Reference:
         self.L = L
         L.ref_threads.restype = C.c_int
         L.ref_uniform_disc.argtypes = [C.c_size_t, C.c_uint, _bodyp]
+        L.ref_two_discs.argtypes = [C.c_size_t, C.c_uint, C.c_float, _bodyp]
         L.ref_iterate.argtypes = [C.c_size_t, _bodyp, C.c_float]
         L.ref_collide.argtypes = [C.c_size_t, _bodyp]
         L.ref_quadtree_forces.argtypes = [C.c_size_t, _bodyp, C.c_float,
@@ -328,6 +354,12 @@ class Reference:
     def uniform_disc(self, n: int, seed: int = 0) -> np.ndarray:
         b = np.zeros(n, BODY_DTYPE)
         self.L.ref_uniform_disc(n, seed, b)
+        return b
+
+    def two_discs(self, n: int, seed: int = 0, approach: float = 0.2) -> np.ndarray:
+        """The two-disc workload from the reference's own uniformDisc."""
+        b = np.zeros(n, BODY_DTYPE)
+        self.L.ref_two_discs(n, seed, approach, b)
         return b
 
     def iterate(self, b, dt):

@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <numeric>
@@ -46,6 +47,33 @@ int ref_threads() {
 void ref_uniform_disc(std::size_t n, unsigned seed, Body *out) {
   std::vector<Body> v = uniformDisc(n, seed);
   std::memcpy(out, v.data(), n * sizeof(Body));
+}
+
+// The two-disc workload built from the reference's own uniformDisc
+// (src/Utils.cpp:6-54) for seeds seed and seed+1: discs of n/2 and n - n/2
+// bodies, centres at (-+3R, 0) with R = 5 sqrt(n/2), bulk velocities
+// (0, +-f v) with v = sqrt(M_total / (6R)), M_total = 2 (1e6 + n/2), the
+// second disc's spin reversed, ids 0..n-1 (the shape of
+// viewer/Scenarios.cpp:36-48).  The timed CPU baseline builds its input
+// here, so that it maps no product code.
+void ref_two_discs(std::size_t n, unsigned seed, float approach, Body *out) {
+  const std::size_t half = n / 2;
+  const float R = 5.0f * std::sqrt(static_cast<float>(half));
+  const float totalMass = 2.0f * (1e6f + static_cast<float>(half));
+  const float v = approach * std::sqrt(totalMass / (6.0f * R));
+  std::size_t k = 0;
+  for (int side = 0; side < 2; ++side) {
+    const std::size_t m = side == 0 ? half : n - half;
+    const float x = side == 0 ? -3.0f * R : 3.0f * R;
+    const float vy = side == 0 ? v : -v;
+    for (Body b : uniformDisc(m, seed + side)) {
+      if (side == 1) b.vel = b.vel * -1.0f;
+      b.pos.x += x;
+      b.vel.y += vy;
+      b.id = k;
+      out[k++] = b;
+    }
+  }
 }
 
 // Body::update for every body (src/Simulation.cpp:44-50).

@@ -62,3 +62,45 @@ def test_gather_metrics_two_ranks():
         p.join(120)
         assert p.exitcode == 0
     assert ret[0] and ret[1]
+
+
+def test_collective_device_follows_backend():
+    sys.path.insert(0, PKG)
+    import torch
+    from ensemble import collective_device
+    assert collective_device("gloo", 3) == torch.device("cpu")
+    assert collective_device("nccl", 3) == torch.device("cuda", 3)
+    assert collective_device("NCCL", 0) == torch.device("cuda", 0)
+
+
+def _nccl_one_rank(port, ret):
+    sys.path.insert(0, PKG)
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from ensemble import gather_metrics
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60),
+                            device_id=torch.device("cuda", 0))
+    local = np.arange(12, dtype=np.float64).reshape(3, 4)
+    full = gather_metrics(dist, [0, 2, 4], local, 5)
+    ok = np.array_equal(full[[0, 2, 4]], local) and np.isnan(full[[1, 3]]).all()
+    dist.destroy_process_group()
+    ret["ok"] = bool(ok)
+
+
+@pytest.mark.gpu
+def test_gather_metrics_on_nccl():
+    """The all-gather through NCCL itself (one rank on the one GPU; the
+    buffers must be CUDA tensors there)."""
+    mgr = mp.Manager()
+    ret = mgr.dict()
+    port = 28500 + os.getpid() % 1000
+    p = mp.get_context("spawn").Process(target=_nccl_one_rank, args=(port, ret))
+    p.start()
+    p.join(180)
+    assert p.exitcode == 0 and ret.get("ok")

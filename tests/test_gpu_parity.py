@@ -165,6 +165,24 @@ def test_collisions_bit_exact(nbx, oracle, golden):
     assert seen_large > 0  # the large-body path saw real contacts
 
 
+def test_collision_stats(nbx, oracle):
+    """Pair count and the longest chain of dependent pairs (each pair waits
+    for the last earlier pair sharing a body) from the oracle's pair list."""
+    st = state(nbx, oracle, "colliding20k")
+    sim = nbx.Simulation(with_central_contacts(st, 8))
+    sim.phase("collide")
+    pairs, depth = sim.collision_stats()
+    ol, oe = oracle.collision_pairs(with_central_contacts(st, 8))
+    last = {}
+    deepest = 0
+    for a, b in zip(ol.tolist(), oe.tolist()):
+        d = max(last.get(a, 0), last.get(b, 0)) + 1
+        last[a] = last[b] = d
+        deepest = max(deepest, d)
+    assert pairs == len(ol) and depth == deepest and depth >= 2
+    sim.close()
+
+
 def test_collide_then_reference_bodies(nbx, golden):
     """Against the reference's own collide() output (fixture)."""
     sim = nbx.Simulation(golden["collide_in"])
@@ -277,6 +295,64 @@ def test_fp64_direct_and_energy(nbx, oracle):
     oem = oracle.energy_momentum(s)
     assert np.allclose(em, oem, rtol=1e-12, atol=1e-9)
     sim.close()
+
+
+def _pair_potential(s, eps, plummer=False):
+    """FP64 pairwise potential in numpy (test-side restatement)."""
+    x = s["px"].astype(np.float64)
+    y = s["py"].astype(np.float64)
+    m = s["mass"].astype(np.float64)
+    dx = x[None, :] - x[:, None]
+    dy = y[None, :] - y[:, None]
+    r2 = dx * dx + dy * dy
+    np.fill_diagonal(r2, np.inf)
+    r = np.sqrt(r2)
+    if plummer:
+        g = 1.0 / np.sqrt(r2 + eps * eps)
+    elif eps > 0:
+        g = np.arctan2(eps, r) / eps
+    else:
+        g = 1.0 / r
+    phi = -(g * m[None, :]).sum(axis=1)
+    return 0.5 * float(np.sum(m * phi)), phi
+
+
+def test_fp64_potential(nbx, oracle):
+    """The potential of the tree law (and of the Plummer law) in FP64:
+    exact over all pairs against the oracle's compensated pair sum, per
+    target against a numpy pair sum, the sampled estimate with every body
+    sampled equal to the exact one, instances summed separately."""
+    b = nbx.uniform_disc(3000)
+    sim = nbx.Simulation(b)
+    sim.step(2)
+    s = sim.download()
+    u = sim.potential()
+    ou = oracle.potential(s, 1.0)
+    assert abs(u - ou) <= 1e-11 * abs(ou), (u, ou)
+    est, phi = sim.potential(np.arange(len(s), dtype=np.uint32))
+    assert abs(est - u) <= 1e-12 * abs(u)
+    nu, nphi = _pair_potential(s, 1.0)
+    assert np.max(np.abs(phi - nphi) / np.abs(nphi)) < 1e-11
+    tg = np.array([0, 7, 2999, 1500], np.uint32)
+    est4, phi4 = sim.potential(tg)
+    assert np.array_equal(phi4, phi[tg])
+    assert abs(est4 - 0.5 * len(s) / 4 * np.sum(s["mass"][tg] * phi4)) <= 1e-12 * abs(est4)
+    sim.close()
+    # two instances: pairs only within each
+    parts = [nbx.uniform_disc(700, 0), nbx.uniform_disc(500, 3)]
+    h = nbx.Handle([700, 500])
+    h.upload(np.concatenate(parts))
+    u2 = h.potential()
+    ref = oracle.potential(parts[0], 1.0) + oracle.potential(parts[1], 1.0)
+    assert abs(u2 - ref) <= 1e-11 * abs(ref)
+    h.close()
+    # Plummer law (force_law 1) and the unsoftened tree law
+    for kw, eps, pl in ((dict(force_law=1), 1.0, True), (dict(epsilon=0.0), 0.0, False)):
+        sm = nbx.Simulation(nbx.uniform_disc(400), **kw)
+        st = sm.download()
+        assert abs(sm.potential() - _pair_potential(st, eps, pl)[0]) <= 1e-11 * abs(
+            _pair_potential(st, eps, pl)[0])
+        sm.close()
 
 
 def test_id_order_download(nbx):

@@ -33,6 +33,18 @@ def test_uniform_disc_matches_reference(nbx, golden):
         assert h == golden[f"disc{n}_sha256"].tobytes(), n
 
 
+def test_reference_arm_input_is_the_products(nbx):
+    """bench.py's reference arm builds the two-disc workload with the
+    reference's own uniformDisc (oracle/_ref), so that it maps no product
+    code; both arms must start from the same bytes."""
+    from oracle import Reference
+    if not Reference.available("omp"):
+        pytest.skip("reference build absent")
+    R = Reference("omp")
+    for n in (4096, 1 << 20):
+        assert same_bits(R.two_discs(n, 0, 0.2), nbx.two_discs(n, 0, 0.2)), n
+
+
 def test_params_default_are_reference_defaults(nbx):
     p = nbx.default_params()
     assert (p.dt, p.theta, p.epsilon, p.leaf_capacity, p.collisions) == (

@@ -45,6 +45,22 @@ def test_noalloc_matches_direct_fp64_twice(nbx):
         gx, gy = ax.cpu().numpy(), ay.cpu().numpy()
         rel = np.hypot(gx - ref_x, gy - ref_y) / np.maximum(np.hypot(ref_x, ref_y), 1e-30)
         assert np.isfinite(rel).all() and rel.max() < 1e-12, (call, rel.max())
+    # targets outside 0..n-1 (they live in device memory, so only the kernel
+    # can tell): not read through, NaN outputs; the in-range ones unchanged
+    tg = np.array([5, n, 17, 0xFFFFFFFF, n - 1], np.uint32)
+    ref_x, ref_y = sim.direct_fp64(tg[[0, 2, 4]])
+    t = torch.from_numpy(tg.view(np.int32)).to(dev)
+    ax = torch.zeros(5, dtype=torch.float64, device=dev)
+    ay = torch.zeros(5, dtype=torch.float64, device=dev)
+    rc = nbx.lib().nbx_direct_fp64_noalloc(
+        x.data_ptr(), y.data_ptr(), m.data_ptr(), n, t.data_ptr(), 5, 1.0,
+        ax.data_ptr(), ay.data_ptr(), stream.cuda_stream)
+    assert rc == 0
+    torch.cuda.synchronize(dev)
+    gx, gy = ax.cpu().numpy(), ay.cpu().numpy()
+    assert np.isnan(gx[[1, 3]]).all() and np.isnan(gy[[1, 3]]).all()
+    rel = np.hypot(gx[[0, 2, 4]] - ref_x, gy[[0, 2, 4]] - ref_y) / np.hypot(ref_x, ref_y)
+    assert rel.max() < 1e-12
     # more targets than the fixed array holds: rejected before any launch
     big = torch.zeros(4097, dtype=torch.int32, device=dev)
     out = torch.zeros(4097, dtype=torch.float64, device=dev)
