@@ -227,9 +227,13 @@ def time_steps(torch, h, stream, steps):
 
 
 def forms_leg(nbx, torch, sim, n, local, ids, args):
-    """Plain theta 0.5 vs the learned correction (and the analytic
-    quadrupole control) on the same state: body-steps/s and the force error
-    against the FP64 direct sum on the same 4096 sampled bodies."""
+    """Plain Barnes-Hut against the learned far-field correction and the
+    analytic quadrupole control on the same state, swept over theta in
+    {0.5, 0.7, 0.9, 1.1} (plus the points nearest plain theta 0.5's cost):
+    body-steps/s and the force error against the FP64 direct sum on the
+    same 4096 sampled bodies.  Also the error floor of the reference's law
+    itself: theta 0 (every body summed with fastInvSqrt, no cells) on 1024 of
+    those bodies."""
     state = sim.download()
     pos = np.empty(n, np.int64)
     pos[state["id"]] = np.arange(n)
@@ -237,13 +241,14 @@ def forms_leg(nbx, torch, sim, n, local, ids, args):
     weights = np.fromfile(WEIGHTS, "<f4")
     steps = max(5, min(args.steps, 200))
     out = []
-    # plain theta 0.5 / 0.45 against the corrected forms at larger theta:
-    # quadrupole theta 0.65 band 0.4 runs at plain 0.5's speed, theta 0.6
-    # band 0.4 beats plain 0.45 on both error and speed
-    for name, theta, use, band in (("plain", 0.5, 0, 0.5), ("plain", 0.45, 0, 0.5),
-                                   ("learned", 0.7, 1, 0.5),
-                                   ("quadrupole", 0.65, 2, 0.4), ("quadrupole", 0.6, 2, 0.4),
-                                   ("quadrupole", 0.55, 2, 0.3)):
+    configs = []
+    for theta in (0.5, 0.7, 0.9, 1.1):
+        configs += [("plain", theta, 0, 0.5), ("learned", theta, 1, 0.5),
+                    ("quadrupole", theta, 2, 0.4)]
+    # the corrected forms nearest plain theta 0.5's cost, and plain 0.45
+    configs += [("plain", 0.45, 0, 0.5), ("quadrupole", 0.65, 2, 0.4),
+                ("quadrupole", 0.6, 2, 0.4), ("quadrupole", 0.55, 2, 0.3)]
+    for name, theta, use, band in configs:
         h = nbx.Simulation(state, theta=theta, use_mlp=use, mlp_band=band, device=local)
         if use == 1:
             h.mlp_set_params(weights)
@@ -256,7 +261,20 @@ def forms_leg(nbx, torch, sim, n, local, ids, args):
                     "body_steps_per_s": n / (ms * 1e-3), "ms_per_step": ms,
                     "p50": err["median"], "p99": err["p99"], "steps": steps})
         h.close()
-    return out
+    # the law's own floor: theta 0 sums every body (with the reference's
+    # fastInvSqrt); against the FP64 law
+    h = nbx.Simulation(state, theta=0.5, device=local)
+    h.phase("build")
+    h.set_params(theta=0.0)
+    t0 = tg[:1024]
+    ax, ay = h.accel_at(state["px"][t0], state["py"][t0])
+    ex, ey = h.direct_fp64(t0)
+    h.close()
+    e = np.hypot(ax - ex, ay - ey) / np.hypot(ex, ey)
+    floor = {"form": "law floor (theta 0: fastInvSqrt law against the FP64 law)",
+             "samples": 1024, "p50": float(np.median(e)),
+             "p99": float(np.percentile(e, 99)), "max": float(e.max())}
+    return {"forms": out, "law_floor": floor}
 
 
 def render_leg(nbx, sim, n):

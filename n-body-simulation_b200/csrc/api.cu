@@ -26,6 +26,8 @@ void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
 void launch_bounds(cudaStream_t s, const DevState &S);
 void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
                   SortScratch &sort);
+void launch_bfs_tree(cudaStream_t s, const DevState &S, ScanScratch &scan,
+                     SortScratch &sort);
 void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
                    const MlpDev *mlp, float band, int corr, bool noClamp);
 void render_vertices(cudaStream_t s, const float4 *pv, const float2 *mr, uint32_t n,
@@ -241,6 +243,7 @@ struct nbx_handle {
   bool timedCapture = false;
   bool uploaded = false;
   bool treeValid = false;   // a Barnes-Hut tree of the current state exists
+  bool bfsValid = false;    // its breadth-first arrays (built on demand)
   bool forceInput = false;  // S.xym holds the current state's bodies
   bool collideValid = false;
   bool idsChecked = false;     // ids verified to be per-instance permutations
@@ -528,6 +531,7 @@ void destroy_graphs(nbx_handle *h) {
 // Flags after a whole step: the naive law builds no tree.
 void after_step(nbx_handle *h) {
   h->treeValid = h->params.force_law == 0;
+  h->bfsValid = false;
   h->forceInput = true;
   h->collideValid = h->params.collisions != 0;
 }
@@ -1286,6 +1290,7 @@ int nbx_phase(nbx_handle *h, int phase) {
     launch_build(s, S, h->scan, h->sort);
     h->cur ^= 1;
     h->treeValid = true;
+    h->bfsValid = false;
     h->forceInput = true;
     break;
   case NBX_PHASE_FORCES:
@@ -1311,6 +1316,7 @@ int nbx_phase(nbx_handle *h, int phase) {
     launch_build(s, S, h->scan, h->sort);
     h->cur ^= 1;
     h->treeValid = true;
+    h->bfsValid = false;
     h->forceInput = true;
     launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
                   h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
@@ -1351,10 +1357,30 @@ static int read_seg(nbx_handle *h, uint32_t inst, SegDev &g) {
   return NBX_OK;
 }
 
+} // extern "C"
+
+// The breadth-first arrays of the last tree, built from its sorted codes
+// the first time they are asked for (the step path builds only the
+// traversal layout).
+static int ensure_bfs_tree(nbx_handle *h) {
+  if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
+  if (h->bfsValid) return NBX_OK;
+  launch_bfs_tree(h->stream, h->state(), h->scan, h->sort);
+  NBX_CUDA(h, cudaGetLastError());
+  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  int rc = check_status(h);
+  if (rc) return rc;
+  h->bfsValid = true;
+  return NBX_OK;
+}
+
+extern "C" {
+
 int nbx_tree_size(nbx_handle *h, uint32_t inst, uint32_t *nodes, uint32_t *levels) {
   if (!h || inst >= h->nseg) return NBX_ERR_ARG;
   cudaSetDevice(h->device);
-  if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
+  int rc0 = ensure_bfs_tree(h);
+  if (rc0) return rc0;
   SegDev g;
   int rc = read_seg(h, inst, g);
   if (rc) return rc;
@@ -1368,7 +1394,8 @@ int nbx_get_tree(nbx_handle *h, uint32_t inst, float *comX, float *comY, float *
                  int32_t *start, int32_t *end, size_t capacity) {
   if (!h || inst >= h->nseg) return NBX_ERR_ARG;
   cudaSetDevice(h->device);
-  if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
+  int rc0 = ensure_bfs_tree(h);
+  if (rc0) return rc0;
   SegDev g;
   int rc = read_seg(h, inst, g);
   if (rc) return rc;

@@ -75,13 +75,12 @@ __global__ void k_root_frame(DevState S) {
   b[3] = 0u;
 }
 
-// Morton code of every body; digit histograms of the radix passes fused
-// (the passes over the high 32 bits: kMortonSortPass0 .. 7).
-constexpr int kMortonSortPass0 = 4;
+// Morton code of every body; the sort key is its high half (depth-16
+// cells), with the digit histograms of its four radix passes fused.
 __global__ void __launch_bounds__(kBlock)
-    k_morton(DevState S, uint64_t *__restrict__ keys, uint32_t *hist) {
-  __shared__ uint32_t sh[8][256];
-  for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) sh[i >> 8][i & 255] = 0;
+    k_morton(DevState S, uint32_t *__restrict__ keys, uint32_t *hist) {
+  __shared__ uint32_t sh[4][256];
+  for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) sh[i >> 8][i & 255] = 0;
   __syncthreads();
   const uint32_t n = S.n;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -89,13 +88,14 @@ __global__ void __launch_bounds__(kBlock)
     const float4 p = S.pv[i];
     const MortonFrame f = S.seg[S.segOf[i]].frame;
     const uint64_t c = morton_code(p.x, p.y, f);
-    keys[i] = c;
+    const uint32_t k = (uint32_t)(c >> 32);
+    keys[i] = k;
     S.codes[i] = c;
 #pragma unroll
-    for (int q = kMortonSortPass0; q < 8; ++q) atomicAdd(&sh[q][(c >> (8 * q)) & 255u], 1u);
+    for (int q = 0; q < 4; ++q) atomicAdd(&sh[q][(k >> (8 * q)) & 255u], 1u);
   }
   __syncthreads();
-  for (int i = kMortonSortPass0 * 256 + threadIdx.x; i < 8 * 256; i += blockDim.x) {
+  for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
     const uint32_t v = sh[i >> 8][i & 255];
     if (v) atomicAdd(&hist[i], v);
   }
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(kBlock)
 
 // Sort key for the instance passes: segment of the element's original index.
 __global__ void k_seg_keys(DevState S, const uint32_t *__restrict__ vals,
-                           uint64_t *__restrict__ keys) {
+                           uint32_t *__restrict__ keys) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n;
        i += gridDim.x * blockDim.x)
     keys[i] = S.segOf[vals[i]];
@@ -209,7 +209,6 @@ __global__ void k_levels(DevState S) {
       }
       G.nodeCount = nodes;
       G.levelCount = levels;
-      G.travCount = 0;
     }
     // block-wide exclusive scan of node counts -> node bases
     __shared__ uint32_t sScan[1024];
@@ -472,53 +471,258 @@ __global__ void __launch_bounds__(kBlock) k_upward(DevState S) {
   }
 }
 
-// Preorder position of every node, and the traversal arrays.
-__global__ void __launch_bounds__(kBlock) k_preorder(DevState S) {
-  const uint32_t total = S.counters[4];
-  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
-       g += gridDim.x * blockDim.x) {
-    const uint32_t sg = seg_of_node(S, g);
-    const SegDev &G = S.seg[sg];
-    const uint32_t nb = G.nodeBase;
-    uint32_t pre = 0;
-    uint32_t cur = g - nb;
-    for (int guard = 0; cur != 0; ++guard) {
-      const uint32_t p = (uint32_t)S.parent[nb + cur];
-      if (p >= G.nodeCount || guard > kMaxDepth) {
+// ------------------------------------------- traversal layout, built directly
+//
+// The force traversal needs only the non-empty nodes, in depth-first
+// preorder, and those follow straight from the sorted codes:
+//  * a node is (first body i, depth d).  The nodes starting at body i have
+//    depths lo_i .. leaf_i: lo_i = lcp(i-1, i) + 1 (0 at an instance's
+//    first body), and leaf_i is the depth of i's leaf.  A node containing
+//    i splits iff it holds more than L bodies, i.e. iff some window
+//    [j, j+L] of the instance around i shares its prefix, so
+//    leaf_i = min(max over j in [i-L, i] of lcp(j, j+L), 31) + 1 (0 when no
+//    window fits);
+//  * in preorder, the nodes starting at i follow every node that starts
+//    before i, shallowest first: with P = the exclusive scan of the counts,
+//    node (i, d) is record P_i + d - lo_i;
+//  * its subtree ends at the first body e past its prefix group, and the
+//    record after the subtree is the first node starting at e, P_e;
+//  * sums go up with arrival counters over the non-empty children in digit
+//    order.  An empty child adds exactly +0 to sums that are never -0 (they
+//    start at +0 and only add), so mass and centre of mass equal
+//    sumNode/finishNode's over all four children (TreeKernels.cuh:150-177)
+//    bit for bit.
+// This replaces the breadth-first arrays on the step path; those are built
+// only when asked for (launch_bfs_tree).
+
+// Nodes starting at each body (splitCount) and the depth of the first one
+// (splitLo).
+__global__ void __launch_bounds__(kBlock) k_trav_counts(DevState S) {
+  const uint64_t *c = S.sortedCodes;
+  const uint32_t L = (uint32_t)S.leafCapacity;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n;
+       i += gridDim.x * blockDim.x) {
+    const SegDev &G = S.seg[S.segOf[i]];
+    const uint32_t s0 = G.start, s1 = G.start + G.count;
+    const uint64_t ci = c[i];
+    const int lo = (i == s0) ? 0 : lcp_digits(c[i - 1], ci) + 1;
+    int w = -1;
+    for (uint32_t j = i >= s0 + L ? i - L : s0; j <= i && (uint64_t)j + L < s1; ++j)
+      w = max(w, min(lcp_digits(c[j], c[j + L]), kMaxDepth - 1));
+    const int leaf = w + 1;
+    S.splitCount[i] = lo <= leaf ? (uint32_t)(leaf - lo + 1) : 0u;
+    S.splitLo[i] = (uint8_t)lo; // <= 33
+  }
+}
+
+// First index in (i, e] whose depth-d prefix differs from code[i]'s (pre),
+// given that the codes from e on all differ (a gallop, then a binary
+// search).  d >= 1.
+__device__ __forceinline__ uint32_t prefix_end(const uint64_t *c, uint32_t i, uint32_t e,
+                                               int d, uint64_t pre) {
+  const int sh = 64 - 2 * d;
+  uint32_t lo = i + 1, hi = e, step = 1;
+  while (lo < hi) {
+    const uint32_t probe = lo + step - 1;
+    if (probe >= hi) break;
+    if ((c[probe] >> sh) != pre) {
+      hi = probe;
+      break;
+    }
+    lo = probe + 1;
+    step <<= 1;
+  }
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if ((c[mid] >> sh) == pre) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// First index in [s0, i] with the depth-d prefix of code[i] (a gallop
+// backwards, then a binary search).  d >= 1.
+__device__ __forceinline__ uint32_t prefix_start(const uint64_t *c, uint32_t s0,
+                                                 uint32_t i, int d) {
+  const int sh = 64 - 2 * d;
+  const uint64_t pre = c[i] >> sh;
+  uint32_t lo = s0, hi = i, step = 1; // answer in [lo, hi]
+  while (hi > lo) {
+    const uint32_t probe = hi - lo >= step ? hi - step : lo;
+    if ((c[probe] >> sh) != pre) {
+      lo = probe + 1;
+      break;
+    }
+    hi = probe;
+    if (probe == lo) break;
+    step <<= 1;
+  }
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if ((c[mid] >> sh) == pre) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+
+// The records of every node: body range, next and open slots, size and
+// centre (splitNode's arithmetic along the path), parent and number of
+// non-empty children; arrival counters cleared.
+__global__ void __launch_bounds__(kBlock) k_trav_nodes(DevState S) {
+  const uint64_t *c = S.sortedCodes;
+  const uint32_t total = S.counters[6];
+  const bool overflow = total > S.nodeCapacity;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t sg = S.segOf[i];
+    SegDev &G = S.seg[sg];
+    const uint32_t s0 = G.start, s1 = G.start + G.count;
+    const uint32_t P = S.splitStart[i];
+    if (i == s0) {
+      // all-or-nothing: no instance gets a traversal, the step reports it
+      G.travBase = overflow ? 0u : P;
+      G.travCount = overflow ? 0u : (s1 < S.n ? S.splitStart[s1] : total) - P;
+      if (overflow && sg == 0) atomicOr(S.status, kStatusTreeCapacity);
+    }
+    const uint32_t cnt = S.splitCount[i];
+    if (overflow || cnt == 0) continue;
+    const int lo = S.splitLo[i];
+    const uint64_t ci = c[i];
+    float cx = G.cx, cy = G.cy, size = G.size;
+    for (int t = 0; t < lo; ++t) {
+      size = __fmul_rn(size, 0.5f);
+      const int q = digit_at(ci, t);
+      cx = __fadd_rn(cx, __fmul_rn((float)(q & 1) - 0.5f, size));
+      cy = __fadd_rn(cy, __fmul_rn((float)(q >> 1) - 0.5f, size));
+    }
+    uint32_t e = s1; // ends shrink with depth
+    for (uint32_t k = 0; k < cnt; ++k) {
+      const int d = lo + (int)k;
+      if (k > 0) {
+        size = __fmul_rn(size, 0.5f);
+        const int q = digit_at(ci, d - 1);
+        cx = __fadd_rn(cx, __fmul_rn((float)(q & 1) - 0.5f, size));
+        cy = __fadd_rn(cy, __fmul_rn((float)(q >> 1) - 0.5f, size));
+      }
+      const uint32_t p = P + k;
+      const bool leaf = k + 1 == cnt;
+      if (d > 0) e = prefix_end(c, i, e, d, ci >> (64 - 2 * d));
+      // the record after the subtree; all ones past the instance's last
+      const uint32_t next = e < s1 ? S.splitStart[e] : 0xffffffffu;
+      int32_t parent = -1;
+      if (d > 0) {
+        if (k > 0) {
+          parent = (int32_t)(p - 1);
+        } else {
+          // the depth-(d-1) node around i starts before it (the root at s0)
+          const uint32_t j = d == 1 ? s0 : prefix_start(c, s0, i, d - 1);
+          parent = (int32_t)(S.splitStart[j] + (uint32_t)(d - 1 - (int)S.splitLo[j]));
+        }
+      }
+      uint32_t children = 0;
+      if (!leaf) {
+        const uint32_t b1 = first_with_digit(c, i, e, d, 1);
+        const uint32_t b2 = first_with_digit(c, b1, e, d, 2);
+        const uint32_t b3 = first_with_digit(c, b2, e, d, 3);
+        children = (b1 > i) + (b2 > b1) + (b3 > b2) + (e > b3);
+      }
+      TravNode &T = S.tN[p];
+      T.a = make_float4(0.0f, 0.0f, 0.0f, __fmul_rn(size, size));
+      T.b = make_int4((int)next, (int)(leaf ? next : p + 1), (int)i, (int)e);
+      S.tM[p] = make_float4(0.0f, 0.0f, 0.0f, size);
+      S.tC[p] = make_float2(cx, cy);
+      S.parent[p] = parent;
+      S.subtree[p] = children;
+      S.arrive[p] = 0u;
+    }
+  }
+}
+
+// Bottom-up sums over the traversal records: each leaf sums its bodies
+// (sumNode's order) and climbs; the last non-empty child to arrive sums its
+// parent's children in digit order, then finishNode's divide; second
+// moments about each centre of mass for the corrected forms.
+__global__ void __launch_bounds__(kBlock) k_trav_upward(DevState S) {
+  const uint32_t total = S.counters[6];
+  if (total > S.nodeCapacity) return;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total;
+       p += gridDim.x * blockDim.x) {
+    const int4 B = S.tN[p].b;
+    if (B.y != B.x) continue; // interior: summed by its last child
+    const uint32_t b0 = (uint32_t)B.z, b1 = min((uint32_t)B.w, S.n);
+    float px = 0.0f, py = 0.0f, mm = 0.0f;
+    for (uint32_t b = b0; b < b1; ++b) {
+      const float4 q = S.xym[b];
+      px = __fadd_rn(px, __fmul_rn(q.x, q.z));
+      py = __fadd_rn(py, __fmul_rn(q.y, q.z));
+      mm = __fadd_rn(mm, q.z);
+    }
+    const float div = fmaxf(mm, FLT_MIN);
+    const float X = __fdiv_rn(px, div), Y = __fdiv_rn(py, div);
+    float ixx = 0.0f, iyy = 0.0f, ixy = 0.0f;
+    for (uint32_t b = b0; b < b1; ++b) {
+      const float4 q = S.xym[b];
+      const float dx = q.x - X, dy = q.y - Y;
+      ixx += q.z * dx * dx;
+      iyy += q.z * dy * dy;
+      ixy += q.z * dx * dy;
+    }
+    __stcg(&S.sumX[p], px);
+    __stcg(&S.sumY[p], py);
+    __stcg(&S.tN[p].a, make_float4(X, Y, mm, S.tN[p].a.w));
+    __stcg(&S.tM[p], make_float4(ixx, iyy, ixy, S.tM[p].w));
+    int32_t node = S.parent[p];
+    for (int guard = 0; node >= 0 && guard <= kMaxDepth; ++guard) {
+      const uint32_t g = (uint32_t)node;
+      if (g >= total) {
         atomicOr(S.status, kStatusTreeCapacity);
-        pre = 0;
         break;
       }
-      const uint32_t cb = (uint32_t)S.children[nb + p];
-      const uint32_t q = cur - cb;
-      pre += 1;
-      for (uint32_t t = 0; t < q; ++t) pre += S.subtree[nb + cb + t];
-      cur = p;
+      const uint32_t children = S.subtree[g];
+      // release: this child's sums are visible to the last arriver;
+      // acquire: the last arriver sees every child's sums
+      uint32_t old;
+      asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;"
+                   : "=r"(old)
+                   : "l"(&S.arrive[g])
+                   : "memory");
+      if (old + 1 != children) break;
+      float sx = 0.0f, sy = 0.0f, sm = 0.0f;
+      uint32_t ch = g + 1;
+      for (uint32_t q = 0; q < children && ch < total; ++q) {
+        const float cxs = __ldcg(&S.sumX[ch]), cys = __ldcg(&S.sumY[ch]);
+        const float cm = __ldcg(&S.tN[ch].a.z);
+        sx = q == 0 ? cxs : __fadd_rn(sx, cxs);
+        sy = q == 0 ? cys : __fadd_rn(sy, cys);
+        sm = q == 0 ? cm : __fadd_rn(sm, cm);
+        ch = (uint32_t)S.tN[ch].b.x;
+      }
+      const float dv = fmaxf(sm, FLT_MIN);
+      const float PX = __fdiv_rn(sx, dv), PY = __fdiv_rn(sy, dv);
+      float jxx = 0.0f, jyy = 0.0f, jxy = 0.0f;
+      ch = g + 1;
+      for (uint32_t q = 0; q < children && ch < total; ++q) {
+        const float4 a = __ldcg(&S.tN[ch].a);
+        const float4 mo = __ldcg(&S.tM[ch]);
+        const float dx = a.x - PX, dy = a.y - PY;
+        jxx += mo.x + a.z * dx * dx;
+        jyy += mo.y + a.z * dy * dy;
+        jxy += mo.z + a.z * dx * dy;
+        ch = (uint32_t)S.tN[ch].b.x;
+      }
+      __stcg(&S.sumX[g], sx);
+      __stcg(&S.sumY[g], sy);
+      __stcg(&S.tN[g].a, make_float4(PX, PY, sm, S.tN[g].a.w));
+      __stcg(&S.tM[g], make_float4(jxx, jyy, jxy, S.tM[g].w));
+      node = S.parent[g];
     }
-    if (g == nb) S.seg[sg].travCount = S.subtree[g];
-    if (S.subtree[g] == 0 || pre >= G.nodeCount) continue; // empty node
-    const uint32_t pg = nb + pre;
-    const float sz = S.size[g];
-    TravNode &T = S.tN[pg];
-    T.a = make_float4(S.comX[g], S.comY[g], S.mass[g], __fmul_rn(sz, sz));
-    // next node after this subtree; all ones past the instance's last node
-    const uint32_t skip = pg + S.subtree[g];
-    const uint32_t nextPg = skip >= nb + S.subtree[nb] ? 0xffffffffu : skip;
-    // where a lane that opens this node goes next: a leaf is summed and
-    // skipped, an interior node descends to its first child (the next
-    // preorder slot)
-    const uint32_t openPg = S.children[g] == 0 ? nextPg : pg + 1;
-    T.b = make_int4((int)nextPg, (int)openPg, (int)(G.start + S.start[g]),
-                    (int)(G.start + S.end[g]));
-    const float4 mo = S.moments[g];
-    S.tM[pg] = make_float4(mo.x, mo.y, mo.z, sz);
-    S.tC[pg] = make_float2(S.centerX[g], S.centerY[g]);
   }
 }
 
 } // namespace
 
 void launch_bounds(cudaStream_t s, const DevState &S);
+void launch_trav_tree(cudaStream_t s, const DevState &S, ScanScratch &scan);
 
 void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
                   SortScratch &sort) {
@@ -526,29 +730,28 @@ void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
   launch_bounds(s, S);
   k_root_frame<<<(S.nseg + 127) / 128, 128, 0, s>>>(S);
   mark(s, "build.bounds");
-  cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * 8 * 256, s);
-  k_morton<<<grid_for(n), kBlock, 0, s>>>(S, sort.keys[0], sort.hist);
+  cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * 4 * 256, s);
+  k_morton<<<grid_for(n), kBlock, 0, s>>>(S, keys32(sort, 0), sort.hist);
   mark(s, "build.morton");
-  // radix passes over the high 32 bits (depth-16 cells), then every run of
-  // equal high bits is ordered by its low bits: the same stable order as a
-  // full 64-bit sort; such runs are rare and short (at most 2 bodies in the
-  // headline states), so this replaces four full passes
-  int buf = radix_sort_u64(s, sort, n, nullptr, 8 * kMortonSortPass0, 64, true, true,
-                           S.status);
-  sort_fix_low_bits(s, sort, buf, n, 8 * kMortonSortPass0, S.longRuns, &S.counters[9],
-                    n / 16 + 64, S.status);
+  // radix passes over the codes' high 32 bits (depth-16 cells), then every
+  // run of equal high bits is ordered by its low bits: the same stable order
+  // as a full 64-bit sort; such runs are rare and short (at most 2 bodies in
+  // the headline states), so this replaces four full passes
+  int buf = radix_sort_u32(s, sort, n, nullptr, 0, 32, true, true, S.status);
+  sort_fix_low_bits32(s, sort, buf, n, S.codes, S.longRuns, &S.counters[9], n / 16 + 64,
+                      S.status);
   mark(s, "build.sort");
   if (S.nseg > 1) {
     // stable passes on the instance id keep instances in their ranges
-    k_seg_keys<<<grid_for(n), kBlock, 0, s>>>(S, sort.vals[buf], sort.keys[buf]);
+    k_seg_keys<<<grid_for(n), kBlock, 0, s>>>(S, sort.vals[buf], keys32(sort, buf));
     if (buf == 1) {
-      cudaMemcpyAsync(sort.keys[0], sort.keys[1], sizeof(uint64_t) * n,
+      cudaMemcpyAsync(keys32(sort, 0), keys32(sort, 1), sizeof(uint32_t) * n,
                       cudaMemcpyDeviceToDevice, s);
       cudaMemcpyAsync(sort.vals[0], sort.vals[1], sizeof(uint32_t) * n,
                       cudaMemcpyDeviceToDevice, s);
     }
     const int segBits = S.nseg <= 256 ? 8 : 16;
-    buf = radix_sort_u64(s, sort, n, nullptr, 0, segBits, false, false, S.status);
+    buf = radix_sort_u32(s, sort, n, nullptr, 0, segBits, false, false, S.status);
   }
   k_gather<<<grid_for(n), kBlock, 0, s>>>(S, sort.vals[buf]);
   mark(s, "build.gather");
@@ -561,28 +764,43 @@ void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
   T.mr2 = S.mr;
   T.id2 = S.id;
   S = T;
-  // tree
+  launch_trav_tree(s, S, scan);
+}
+
+// The traversal layout straight from the sorted codes (the step path).
+void launch_trav_tree(cudaStream_t s, const DevState &S, ScanScratch &scan) {
+  const uint32_t n = S.n;
+  k_trav_counts<<<grid_for(n), kBlock, 0, s>>>(S);
+  exclusive_scan_u32(s, S.splitCount, S.splitStart, n, nullptr, &S.counters[6],
+                     scan, S.status);
+  mark(s, "tree.counts");
+  k_trav_nodes<<<grid_for(n), kBlock, 0, s>>>(S);
+  mark(s, "tree.nodes");
+  k_trav_upward<<<grid_for(n / 4 + 64), kBlock, 0, s>>>(S);
+  mark(s, "tree.upward");
+}
+
+// The reference's breadth-first node arrays (TreeKernels.cuh:88-95) of the
+// last build, for introspection only: the step path does not need them.
+// Uses the per-body split scratch and the sort scratch, and leaves the
+// traversal layout as it is.
+void launch_bfs_tree(cudaStream_t s, const DevState &S, ScanScratch &scan,
+                     SortScratch &sort) {
+  const uint32_t n = S.n;
   k_split_counts<<<grid_for(n), kBlock, 0, s>>>(S);
   exclusive_scan_u32(s, S.splitCount, S.splitStart, n, nullptr, &S.counters[3],
                      scan, S.status);
   k_split_emit<<<grid_for(n), kBlock, 0, s>>>(S, sort.keys[0], sort.vals[0]);
   const int depthBits = S.nseg <= 4 ? 8 : (S.nseg <= 1024 ? 16 : 24);
-  mark(s, "tree.split_emit");
   const int eb = radix_sort_u64(s, sort, 2 * n + 64, &S.counters[3], 0,
                                 depthBits, false, false, S.status);
-  mark(s, "tree.entry_sort");
   cudaMemsetAsync(S.groupStart, 0, sizeof(uint32_t) * S.nseg * kLevelSlots, s);
   cudaMemsetAsync(S.groupEnd, 0, sizeof(uint32_t) * S.nseg * kLevelSlots, s);
   k_groups<<<grid_for(2 * n), kBlock, 0, s>>>(S, sort.keys[eb]);
   k_levels<<<1, 1024, 0, s>>>(S);
-  mark(s, "tree.levels");
   k_split_nodes<<<grid_for(n / 4 + 64), kBlock, 0, s>>>(S, sort.keys[eb],
                                                         sort.vals[eb]);
-  mark(s, "tree.split_nodes");
   k_upward<<<grid_for(n), kBlock, 0, s>>>(S);
-  mark(s, "tree.upward");
-  k_preorder<<<grid_for(n), kBlock, 0, s>>>(S);
-  mark(s, "tree.preorder");
 }
 
 } // namespace nbx

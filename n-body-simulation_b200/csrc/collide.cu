@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_large(DevState S) {
 
 // Units (bodies that are the later box of >= 1 pair), in index order, keyed
 // by their minX for the before()-order sort.
-__global__ void __launch_bounds__(kBlock) k_units(DevState S, uint64_t *keys,
+__global__ void __launch_bounds__(kBlock) k_units(DevState S, uint32_t *keys,
                                                   uint32_t *vals) {
   const uint32_t n = S.n;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -697,8 +697,8 @@ void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
   // units in before() order
   exclusive_scan_u32(s, S.unitFlag, S.unitPos, n, nullptr, &S.counters[1],
                      scan, S.status);
-  k_units<<<grid_for(n), kBlock, 0, s>>>(S, sort.keys[0], sort.vals[0]);
-  const int buf = radix_sort_u64(s, sort, n, &S.counters[1], 0, 32, false,
+  k_units<<<grid_for(n), kBlock, 0, s>>>(S, keys32(sort, 0), sort.vals[0]);
+  const int buf = radix_sort_u32(s, sort, n, &S.counters[1], 0, 32, false,
                                  false, S.status);
   mark(s, "collide.units");
   // ordered resolution

@@ -236,6 +236,125 @@ __device__ __forceinline__ void walk_targets(
   }
 }
 
+// Paired FP32 arithmetic (sm_100 f32x2: one instruction for two lanes of
+// float math in a 64-bit register pair).
+typedef unsigned long long f2x;
+__device__ __forceinline__ f2x pk2(float a, float b) {
+  f2x r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void upk2(f2x r, float &a, float &b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+__device__ __forceinline__ f2x add2(f2x a, f2x b) {
+  f2x r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2x sub2(f2x a, f2x b) {
+  f2x r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2x mul2(f2x a, f2x b) {
+  f2x r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2x fma2(f2x a, f2x b, f2x c) {
+  f2x r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
+// The default plain walk (contracted arithmetic, clamp-free law, no
+// correction, no counting) with paired FP32 instructions: the cell term's
+// {dx, dy} and its accumulation are one pair each, and a leaf's bodies are
+// taken two at a time (structure-of-arrays staging, so one 64-bit shared
+// load gives two bodies' x, y or mass).  Each body accepts, opens and skips
+// exactly the nodes walk_targets does, and every term is the same float
+// arithmetic; only the leaf terms' summation order changes (two running
+// sums, added to the cell terms at the end).
+__device__ __forceinline__ void walk_plain_x2(const DevState &S, float tSq, float eSq,
+                                              float x, float y, uint32_t cur,
+                                              float *sX, float *sY, float *sM,
+                                              float &axOut, float &ayOut) {
+  const int lane = threadIdx.x & 31;
+  const f2x P = pk2(x, y), XX = pk2(x, x), YY = pk2(y, y), E2 = pk2(eSq, eSq);
+  const f2x NHALF = pk2(-0.5f, -0.5f), THREEHALF = pk2(1.5f, 1.5f);
+  f2x acc = pk2(0.0f, 0.0f);  // cell terms {ax, ay}
+  f2x lx = pk2(0.0f, 0.0f), ly = pk2(0.0f, 0.0f); // leaf terms, two sums each
+  for (;;) {
+    const uint32_t k = __reduce_min_sync(0xffffffffu, cur);
+    if (k == kDone) break;
+    float4 A;
+    int4 B;
+    ld_node(&S.tN[k], A, B);
+    const uint32_t nxt = (uint32_t)B.x;
+    const bool at = cur == k;
+    const f2x D = sub2(pk2(A.x, A.y), P);
+    float dx, dy;
+    upk2(D, dx, dy);
+    const float dSq = fmaf(dx, dx, dy * dy);
+    const bool accept = at && A.w < dSq * tSq;
+    const bool openLeaf = at && !accept && B.y == B.x; // leaf: open == next
+    // a massless cell adds exactly +-0 in the clamp-free law (masses >= 0,
+    // finite terms), so no mass test
+    float fac = A.z * fast_inv_sqrt(dSq) * rcp_approx(dSq + eSq);
+    fac = accept ? fac : 0.0f;
+    acc = fma2(D, pk2(fac, fac), acc);
+    cur = at ? (accept ? nxt : (uint32_t)B.y) : cur;
+    if (__ballot_sync(0xffffffffu, openLeaf)) {
+      const uint32_t b0 = (uint32_t)B.z, b1 = (uint32_t)B.w;
+      const uint32_t bEnd = b1 <= S.n ? b1 : S.n; // defensive bound
+      for (uint32_t base = b0; base < bEnd; base += 32) {
+        const uint32_t cnt = min(32u, bEnd - base);
+        __syncwarp();
+        if ((uint32_t)lane < cnt) {
+          const float4 q = S.xym[base + lane];
+          sX[lane] = q.x;
+          sY[lane] = q.y;
+          sM[lane] = q.z;
+        } else if ((uint32_t)lane == cnt) { // odd count: a massless partner
+          sX[lane] = 0.0f;
+          sY[lane] = 0.0f;
+          sM[lane] = 0.0f;
+        }
+        __syncwarp();
+        if (openLeaf) {
+          const uint32_t pairs = (cnt + 1) >> 1;
+          for (uint32_t p = 0; p < pairs; ++p) {
+            const f2x X2 = reinterpret_cast<const f2x *>(sX)[p];
+            const f2x Y2 = reinterpret_cast<const f2x *>(sY)[p];
+            const f2x M2 = reinterpret_cast<const f2x *>(sM)[p];
+            const f2x EX = sub2(X2, XX), EY = sub2(Y2, YY);
+            const f2x D2 = fma2(EX, EX, mul2(EY, EY));
+            float d0, d1;
+            upk2(D2, d0, d1);
+            // fastInvSqrt of both: magic guess, one Newton step
+            const f2x G = pk2(u2f(0x5f3759dfu - (f2u(d0) >> 1)),
+                              u2f(0x5f3759dfu - (f2u(d1) >> 1)));
+            const f2x T = mul2(mul2(D2, NHALF), G);
+            const f2x IS = mul2(G, fma2(T, G, THREEHALF));
+            float q0, q1;
+            upk2(add2(D2, E2), q0, q1);
+            const f2x F = mul2(mul2(M2, IS), pk2(rcp_approx(q0), rcp_approx(q1)));
+            lx = fma2(EX, F, lx);
+            ly = fma2(EY, F, ly);
+          }
+        }
+      }
+    }
+  }
+  float ax, ay, lx0, lx1, ly0, ly1;
+  upk2(acc, ax, ay);
+  upk2(lx, lx0, lx1);
+  upk2(ly, ly0, ly1);
+  axOut = ax + (lx0 + lx1);
+  ayOut = ay + (ly0 + ly1);
+}
+
 // Every target of the launch, one warp per 32.
 template <bool kExact, bool kCount, int kCorr, bool kClamp>
 __device__ __forceinline__ void forces_walk(
@@ -266,18 +385,23 @@ __device__ __forceinline__ void forces_walk(
         y = b.y;
       }
       const SegDev &G = S.seg[query ? 0u : S.segOf[i]];
-      if (G.travCount > 0) cur = G.nodeBase;
+      if (G.travCount > 0) cur = G.travBase;
       wide = G.wide != 0u;
     }
     float ax = 0.0f, ay = 0.0f;
     uint32_t nFar = 0, nNear = 0, nVisit = 0, nIter = 0, nChunk = 0;
     // the clamp-free law only while no lane's instance reaches beyond the
     // coordinate limit (the build's per-instance flag)
-    if (!kClamp && __any_sync(0xffffffffu, wide))
+    constexpr bool kPlainX2 = !kExact && !kCount && kCorr == 0 && !kClamp;
+    const bool anyWide = !kClamp && __any_sync(0xffffffffu, wide);
+    if (anyWide)
       walk_targets<kExact, kCount, kCorr, true>(S, tSq, eSq, bandSq, eps, x, y, cur,
                                                 sBody[w], sW, sStage[kCorr == 1 ? w : 0],
                                                 ax, ay, nFar, nNear, nVisit, nIter, nChunk);
-    else
+    else if (kPlainX2) {
+      float *sX = reinterpret_cast<float *>(sBody[w]);
+      walk_plain_x2(S, tSq, eSq, x, y, cur, sX, sX + 32, sX + 64, ax, ay);
+    } else
       walk_targets<kExact, kCount, kCorr, kClamp>(S, tSq, eSq, bandSq, eps, x, y, cur,
                                                   sBody[w], sW, sStage[kCorr == 1 ? w : 0],
                                                   ax, ay, nFar, nNear, nVisit, nIter, nChunk);

@@ -38,7 +38,7 @@ __global__ void k_harvest_walk(DevState S, const uint32_t *__restrict__ targets,
     const uint32_t t = targets[q];
     const float4 P = S.xym[t];
     const SegDev &G = S.seg[S.segOf[t]];
-    uint32_t cur = G.nodeBase, end = G.nodeBase + G.travCount;
+    uint32_t cur = G.travBase, end = G.travBase + G.travCount;
     uint32_t guard = 0;
     while (cur < end && ++guard < (1u << 24)) {
       const float4 A = S.tN[cur].a;

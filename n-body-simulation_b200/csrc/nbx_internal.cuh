@@ -127,8 +127,6 @@ struct SortScratch {
 };
 
 size_t sort_tiles(uint32_t n_max);
-void sort_fix_low_bits(cudaStream_t s, SortScratch &sc, int buf, uint32_t n, int shift,
-                       uint32_t *longRuns, uint32_t *runCount, uint32_t cap, uint32_t *err);
 
 // Stable LSD radix sort of (keys[0], vals[0]) on key bits [bit_lo, bit_hi)
 // (multiples of 8).  If `have_hist` the caller already filled
@@ -140,9 +138,21 @@ int radix_sort_u64(cudaStream_t s, SortScratch &sc, uint32_t n_max,
                    const uint32_t *d_n, int bit_lo, int bit_hi,
                    bool vals_identity, bool have_hist, uint32_t *err);
 
-// Digit histograms of keys for passes [bit_lo, bit_hi) (zeroes them first).
-void radix_histogram(cudaStream_t s, SortScratch &sc, const uint64_t *keys,
-                     uint32_t n_max, const uint32_t *d_n, int bit_lo,
-                     int bit_hi);
+// The same sort with 32-bit keys, held in the key buffers' storage
+// (keys32): two thirds of the bytes per pass of 64-bit keys.
+inline uint32_t *keys32(SortScratch &sc, int buf) {
+  return reinterpret_cast<uint32_t *>(sc.keys[buf]);
+}
+int radix_sort_u32(cudaStream_t s, SortScratch &sc, uint32_t n_max,
+                   const uint32_t *d_n, int bit_lo, int bit_hi,
+                   bool vals_identity, bool have_hist, uint32_t *err);
+
+// Completes a stable sort of 64-bit codes that ran its radix passes on the
+// high 32 bits only (keys32(sc, buf) = codes[vals] >> 32, sorted): every run
+// of equal keys is put in order of the low 32 bits of codes[vals], stably,
+// in place.  longRuns holds cap run starts; *runCount is device scratch.
+void sort_fix_low_bits32(cudaStream_t s, SortScratch &sc, int buf, uint32_t n,
+                         const uint64_t *codes, uint32_t *longRuns, uint32_t *runCount,
+                         uint32_t cap, uint32_t *err);
 
 } // namespace nbx

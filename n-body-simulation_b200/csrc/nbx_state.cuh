@@ -16,12 +16,14 @@ struct SegDev {
   float cx, cy, size; // root square (Quad::newContaining)
   uint32_t pad1;
   MortonFrame frame;  // quantisation constants (binary64 bit patterns)
-  uint32_t nodeBase;  // first node of this segment's tree
+  uint32_t nodeBase;  // first node of this segment's tree (breadth-first
+                      // arrays, the reference's numbering)
   uint32_t nodeCount; // nodes in this segment's tree
   uint32_t levelCount;
   uint32_t largeStart, largeCount;
   uint32_t travCount; // nodes in the traversal layout (non-empty nodes)
-  uint32_t pad2[2];
+  uint32_t travBase;  // first record of this segment's traversal layout
+  uint32_t pad2;
 };
 
 // A node of the force traversal, in depth-first preorder: a = {comX, comY,
@@ -103,7 +105,8 @@ struct DevState {
   uint32_t *longRuns;    // Morton sort: starts of runs of > 16 equal high keys
   uint32_t *counters;    // [0]=pairs*2 total [1]=units [2]=unit claim
                          // [3]=splitting entries [4]=total nodes
-                         // [5]=small-large pairs [8]=id check
+                         // [5]=small-large pairs [6]=traversal records
+                         // [8]=id check
                          // [9]=long Morton runs [12]=upload mass bits
                          // [13]=expiry test flag [kCtrCoordLimit] (above)
 

@@ -139,7 +139,8 @@ namespace {
 constexpr uint32_t kRFlagShift = 30;
 constexpr uint32_t kRValueMask = (1u << 30) - 1;
 
-__global__ void k_radix_hist(const uint64_t *__restrict__ keys, uint32_t n_max,
+template <typename K>
+__global__ void k_radix_hist(const K *__restrict__ keys, uint32_t n_max,
                              const uint32_t *d_n, int pass_lo, int passes,
                              uint32_t *__restrict__ hist) {
   __shared__ uint32_t sh[8][256];
@@ -149,7 +150,7 @@ __global__ void k_radix_hist(const uint64_t *__restrict__ keys, uint32_t n_max,
   const uint32_t n = load_count(d_n, n_max);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += gridDim.x * blockDim.x) {
-    const uint64_t k = keys[i];
+    const K k = keys[i];
     for (int p = 0; p < passes; ++p)
       atomicAdd(&sh[p][(k >> (8 * (pass_lo + p))) & 255u], 1u);
   }
@@ -176,15 +177,15 @@ __global__ void k_radix_hist_scan(uint32_t *hist, int pass_lo) {
   h[t] = s[t] - h[t];
 }
 
-template <bool kIdentity>
+template <typename K, bool kIdentity>
 __global__ void __launch_bounds__(kSortThreads)
-    k_onesweep(const uint64_t *__restrict__ keysIn,
+    k_onesweep(const K *__restrict__ keysIn,
                const uint32_t *__restrict__ valsIn,
-               uint64_t *__restrict__ keysOut, uint32_t *__restrict__ valsOut,
+               K *__restrict__ keysOut, uint32_t *__restrict__ valsOut,
                const uint32_t *__restrict__ digitStart, uint32_t *status,
                uint32_t *tileCounter, uint32_t n_max, const uint32_t *d_n,
                int shift, uint32_t *err) {
-  __shared__ uint64_t s_keys[kSortTile];
+  __shared__ K s_keys[kSortTile];
   __shared__ uint32_t s_vals[kSortTile];
   __shared__ uint32_t s_whist[kSortWarps][256];
   __shared__ uint32_t s_local[256];  // local exclusive digit start in tile
@@ -202,7 +203,7 @@ __global__ void __launch_bounds__(kSortThreads)
   const uint32_t base = tile * kSortTile;
   const uint32_t wbase = base + warp * (kSortItems * 32);
 
-  uint64_t key[kSortItems];
+  K key[kSortItems];
   uint32_t val[kSortItems];
   uint32_t rank[kSortItems];
   uint32_t dig[kSortItems];
@@ -210,7 +211,7 @@ __global__ void __launch_bounds__(kSortThreads)
   for (int k = 0; k < kSortItems; ++k) {
     const uint32_t i = wbase + k * 32 + lane;
     const bool ok = i < n;
-    key[k] = ok ? keysIn[i] : 0ull;
+    key[k] = ok ? keysIn[i] : (K)0;
     val[k] = ok ? (kIdentity ? i : valsIn[i]) : 0u;
     dig[k] = ok ? (uint32_t)((key[k] >> shift) & 255u) : 256u;
   }
@@ -330,7 +331,7 @@ __global__ void __launch_bounds__(kSortThreads)
   __syncthreads();
   const uint32_t valid = min((uint32_t)kSortTile, n - base);
   for (uint32_t p = tid; p < valid; p += kSortThreads) {
-    const uint64_t k = s_keys[p];
+    const K k = s_keys[p];
     const uint32_t d = (uint32_t)((k >> shift) & 255u);
     const uint32_t dest = s_global[d] + (p - s_local[d]);
     keysOut[dest] = k;
@@ -340,61 +341,56 @@ __global__ void __launch_bounds__(kSortThreads)
 
 constexpr uint32_t kShortRun = 16; // runs up to this length: one thread
 
-// Keys sorted (stably) by their bits >= shift only: every run of equal high
-// bits is put in order of its low bits, stably, in place.  Runs of up to
-// kShortRun keys are insertion-sorted by the thread at their start; longer
-// ones are listed for k_long_runs.  Reordering inside a run never changes
-// the high bits the other threads compare, so run detection is unaffected.
+// 32-bit keys (the high halves of 64-bit codes): every run of equal keys is
+// put in order of the codes' low halves, stably, in place in vals.  Runs of
+// up to kShortRun are insertion-sorted by the thread at their start; longer
+// ones are listed for k_long_runs32.
 __global__ void __launch_bounds__(256)
-    k_fix_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t n,
-               int shift, uint32_t *__restrict__ longRuns, uint32_t *longCount,
-               uint32_t cap, uint32_t *err) {
+    k_fix_runs32(const uint32_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                 uint32_t n, const uint64_t *__restrict__ codes,
+                 uint32_t *__restrict__ longRuns, uint32_t *longCount, uint32_t cap,
+                 uint32_t *err) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += gridDim.x * blockDim.x) {
-    const uint64_t hi = keys[i] >> shift;
-    if (i > 0 && (keys[i - 1] >> shift) == hi) continue; // not a run start
-    if (i + 1 >= n || (keys[i + 1] >> shift) != hi) continue; // single key
+    const uint32_t hi = keys[i];
+    if (i > 0 && keys[i - 1] == hi) continue;      // not a run start
+    if (i + 1 >= n || keys[i + 1] != hi) continue; // single key
     uint32_t len = 2;
-    while (i + len < n && len <= kShortRun && (keys[i + len] >> shift) == hi) ++len;
+    while (i + len < n && len <= kShortRun && keys[i + len] == hi) ++len;
     if (len > kShortRun) {
       const uint32_t slot = atomicAdd(longCount, 1u);
       if (slot < cap) longRuns[slot] = i;
       else atomicOr(err, kStatusSpinLimit);
       continue;
     }
-    uint64_t k[kShortRun];
-    uint32_t v[kShortRun];
+    uint32_t lk[kShortRun], v[kShortRun];
     for (uint32_t a = 0; a < len; ++a) {
-      k[a] = keys[i + a];
       v[a] = vals[i + a];
+      lk[a] = (uint32_t)codes[v[a]];
     }
     for (uint32_t a = 1; a < len; ++a) { // stable: equal keys keep their order
-      const uint64_t kk = k[a];
-      const uint32_t vv = v[a];
+      const uint32_t kk = lk[a], vv = v[a];
       uint32_t b = a;
-      while (b > 0 && k[b - 1] > kk) {
-        k[b] = k[b - 1];
+      while (b > 0 && lk[b - 1] > kk) {
+        lk[b] = lk[b - 1];
         v[b] = v[b - 1];
         --b;
       }
-      k[b] = kk;
+      lk[b] = kk;
       v[b] = vv;
     }
-    for (uint32_t a = 0; a < len; ++a) {
-      keys[i + a] = k[a];
-      vals[i + a] = v[a];
-    }
+    for (uint32_t a = 0; a < len; ++a) vals[i + a] = v[a];
   }
 }
 
-// One block per long run: a stable LSD radix sort of the run on its bits
-// below `shift` (shift / 8 passes through tmp, which holds the same index
-// range), tile by tile in input order so equal digits keep their order.
+// One block per long run: its keys are replaced by the codes' low halves, a
+// stable LSD radix sort (4 passes, through the other buffer over the same
+// index range) orders the run, and the keys are restored.
 __global__ void __launch_bounds__(256)
-    k_long_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ vals,
-                uint64_t *__restrict__ tmpK, uint32_t *__restrict__ tmpV, uint32_t n,
-                int shift, const uint32_t *__restrict__ longRuns, const uint32_t *longCount,
-                uint32_t cap) {
+    k_long_runs32(uint32_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                  uint32_t *__restrict__ tmpK, uint32_t *__restrict__ tmpV, uint32_t n,
+                  const uint64_t *__restrict__ codes, const uint32_t *__restrict__ longRuns,
+                  const uint32_t *longCount, uint32_t cap) {
   __shared__ uint32_t sHist[256], sOff[256], sWarp[8][256];
   __shared__ uint32_t sEnd;
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -402,27 +398,26 @@ __global__ void __launch_bounds__(256)
   const uint32_t ltmask = lanemask_lt();
   for (uint32_t r = blockIdx.x; r < runs; r += gridDim.x) {
     const uint32_t s0 = longRuns[r];
-    const uint64_t hi = keys[s0] >> shift;
-    // run end: the first key past s0 with other high bits
+    const uint32_t hi = keys[s0];
     if (tid == 0) sEnd = n;
     __syncthreads();
     for (uint32_t base = s0; base < n; base += 256) {
       const uint32_t i = base + tid;
-      if (i < n && (keys[i] >> shift) != hi) atomicMin(&sEnd, i);
+      if (i < n && keys[i] != hi) atomicMin(&sEnd, i);
       __syncthreads();
       const bool found = sEnd != n;
       __syncthreads(); // every thread has read sEnd before the next tile
       if (found) break;
     }
     const uint32_t e0 = sEnd;
-    uint64_t *srcK = keys, *dstK = tmpK;
-    uint32_t *srcV = vals, *dstV = tmpV;
-    for (int p = 0; p * 8 < shift; ++p) {
+    for (uint32_t i = s0 + tid; i < e0; i += 256) keys[i] = (uint32_t)codes[vals[i]];
+    __syncthreads();
+    uint32_t *srcK = keys, *dstK = tmpK, *srcV = vals, *dstV = tmpV;
+    for (int p = 0; p < 4; ++p) {
       const int sh = 8 * p;
       sHist[tid] = 0;
       __syncthreads();
-      for (uint32_t i = s0 + tid; i < e0; i += 256)
-        atomicAdd(&sHist[(uint32_t)(srcK[i] >> sh) & 255u], 1u);
+      for (uint32_t i = s0 + tid; i < e0; i += 256) atomicAdd(&sHist[(srcK[i] >> sh) & 255u], 1u);
       __syncthreads();
       if (tid == 0) {
         uint32_t run = s0;
@@ -435,9 +430,9 @@ __global__ void __launch_bounds__(256)
       for (uint32_t base = s0; base < e0; base += 256) {
         const uint32_t i = base + tid;
         const bool ok = i < e0;
-        const uint64_t k = ok ? srcK[i] : 0ull;
+        const uint32_t k = ok ? srcK[i] : 0u;
         const uint32_t v = ok ? srcV[i] : 0u;
-        const uint32_t d = ok ? ((uint32_t)(k >> sh) & 255u) : 256u;
+        const uint32_t d = ok ? ((k >> sh) & 255u) : 256u;
         uint32_t peers = __ballot_sync(0xffffffffu, ok);
 #pragma unroll
         for (int bit = 0; bit < 8; ++bit) {
@@ -448,7 +443,6 @@ __global__ void __launch_bounds__(256)
         __syncthreads();
         if (ok && __popc(peers & ltmask) == 0) sWarp[warp][d] = __popc(peers);
         __syncthreads();
-        // exclusive prefix over warps per digit, tile total into the offsets
         {
           uint32_t acc = 0;
           for (int w = 0; w < 8; ++w) {
@@ -468,61 +462,51 @@ __global__ void __launch_bounds__(256)
         sOff[tid] += sHist[tid];
         __syncthreads();
       }
-      uint64_t *tk = srcK;
+      uint32_t *tk = srcK;
       srcK = dstK;
       dstK = tk;
       uint32_t *tv = srcV;
       srcV = dstV;
       dstV = tv;
     }
-    if (srcK != keys) { // odd number of passes: copy back
-      for (uint32_t i = s0 + tid; i < e0; i += 256) {
-        keys[i] = srcK[i];
-        vals[i] = srcV[i];
-      }
-    }
+    // four passes: the result is back in keys/vals; restore the run's keys
+    for (uint32_t i = s0 + tid; i < e0; i += 256) keys[i] = hi;
     __syncthreads();
   }
 }
 
 } // namespace
 
-// Completes a sort that ran its radix passes on the bits >= shift only:
-// orders every run of equal high bits by the low bits (stable), in place in
-// sc.keys[buf] / sc.vals[buf].  longRuns holds cap run starts; *runCount is
-// device scratch.
-void sort_fix_low_bits(cudaStream_t s, SortScratch &sc, int buf, uint32_t n, int shift,
-                       uint32_t *longRuns, uint32_t *runCount, uint32_t cap, uint32_t *err) {
+void sort_fix_low_bits32(cudaStream_t s, SortScratch &sc, int buf, uint32_t n,
+                         const uint64_t *codes, uint32_t *longRuns, uint32_t *runCount,
+                         uint32_t cap, uint32_t *err) {
   if (n < 2) return;
   cudaMemsetAsync(runCount, 0, sizeof(uint32_t), s);
   uint32_t b = (n + 255) / 256;
   if (b > 148u * 16u) b = 148u * 16u;
-  k_fix_runs<<<b, 256, 0, s>>>(sc.keys[buf], sc.vals[buf], n, shift, longRuns, runCount,
-                               cap, err);
-  k_long_runs<<<148, 256, 0, s>>>(sc.keys[buf], sc.vals[buf], sc.keys[buf ^ 1],
-                                   sc.vals[buf ^ 1], n, shift, longRuns, runCount, cap);
+  k_fix_runs32<<<b, 256, 0, s>>>(keys32(sc, buf), sc.vals[buf], n, codes, longRuns, runCount,
+                                 cap, err);
+  k_long_runs32<<<148, 256, 0, s>>>(keys32(sc, buf), sc.vals[buf], keys32(sc, buf ^ 1),
+                                     sc.vals[buf ^ 1], n, codes, longRuns, runCount, cap);
 }
 
 size_t sort_tiles(uint32_t n_max) {
   return (n_max + kSortTile - 1) / kSortTile + 1;
 }
 
-void radix_histogram(cudaStream_t s, SortScratch &sc, const uint64_t *keys,
-                     uint32_t n_max, const uint32_t *d_n, int bit_lo,
-                     int bit_hi) {
+namespace {
+template <typename K>
+int radix_sort(cudaStream_t s, SortScratch &sc, K *const keys[2], uint32_t n_max,
+               const uint32_t *d_n, int bit_lo, int bit_hi, bool vals_identity,
+               bool have_hist, uint32_t *err) {
   const int p0 = bit_lo / 8, np = (bit_hi - bit_lo) / 8;
-  cudaMemsetAsync(sc.hist + p0 * 256, 0, sizeof(uint32_t) * 256 * np, s);
-  int blocks = (int)((n_max + 1023) / 1024);
-  if (blocks > 1184) blocks = 1184;
-  if (blocks < 1) blocks = 1;
-  k_radix_hist<<<blocks, 256, 0, s>>>(keys, n_max, d_n, p0, np, sc.hist);
-}
-
-int radix_sort_u64(cudaStream_t s, SortScratch &sc, uint32_t n_max,
-                   const uint32_t *d_n, int bit_lo, int bit_hi,
-                   bool vals_identity, bool have_hist, uint32_t *err) {
-  const int p0 = bit_lo / 8, np = (bit_hi - bit_lo) / 8;
-  if (!have_hist) radix_histogram(s, sc, sc.keys[0], n_max, d_n, bit_lo, bit_hi);
+  if (!have_hist) {
+    cudaMemsetAsync(sc.hist + p0 * 256, 0, sizeof(uint32_t) * 256 * np, s);
+    int blocks = (int)((n_max + 1023) / 1024);
+    if (blocks > 1184) blocks = 1184;
+    if (blocks < 1) blocks = 1;
+    k_radix_hist<K><<<blocks, 256, 0, s>>>(keys[0], n_max, d_n, p0, np, sc.hist);
+  }
   k_radix_hist_scan<<<np, 256, 0, s>>>(sc.hist, p0);
   const uint32_t tiles = (n_max + kSortTile - 1) / kSortTile;
   cudaMemsetAsync(sc.tileCounter, 0, sizeof(uint32_t) * 8, s);
@@ -534,19 +518,35 @@ int radix_sort_u64(cudaStream_t s, SortScratch &sc, uint32_t n_max,
     uint32_t *status = sc.status + passWords * p;
     const int shift = 8 * (p0 + p);
     if (p == 0 && vals_identity) {
-      k_onesweep<true><<<tiles > 0 ? tiles : 1, kSortThreads, 0, s>>>(
-          sc.keys[cur], sc.vals[cur], sc.keys[cur ^ 1], sc.vals[cur ^ 1],
+      k_onesweep<K, true><<<tiles > 0 ? tiles : 1, kSortThreads, 0, s>>>(
+          keys[cur], sc.vals[cur], keys[cur ^ 1], sc.vals[cur ^ 1],
           sc.hist + (p0 + p) * 256, status, sc.tileCounter + p, n_max, d_n,
           shift, err);
     } else {
-      k_onesweep<false><<<tiles > 0 ? tiles : 1, kSortThreads, 0, s>>>(
-          sc.keys[cur], sc.vals[cur], sc.keys[cur ^ 1], sc.vals[cur ^ 1],
+      k_onesweep<K, false><<<tiles > 0 ? tiles : 1, kSortThreads, 0, s>>>(
+          keys[cur], sc.vals[cur], keys[cur ^ 1], sc.vals[cur ^ 1],
           sc.hist + (p0 + p) * 256, status, sc.tileCounter + p, n_max, d_n,
           shift, err);
     }
     cur ^= 1;
   }
   return cur;
+}
+} // namespace
+
+int radix_sort_u64(cudaStream_t s, SortScratch &sc, uint32_t n_max,
+                   const uint32_t *d_n, int bit_lo, int bit_hi,
+                   bool vals_identity, bool have_hist, uint32_t *err) {
+  return radix_sort<uint64_t>(s, sc, sc.keys, n_max, d_n, bit_lo, bit_hi, vals_identity,
+                              have_hist, err);
+}
+
+int radix_sort_u32(cudaStream_t s, SortScratch &sc, uint32_t n_max,
+                   const uint32_t *d_n, int bit_lo, int bit_hi,
+                   bool vals_identity, bool have_hist, uint32_t *err) {
+  uint32_t *const keys[2] = {keys32(sc, 0), keys32(sc, 1)};
+  return radix_sort<uint32_t>(s, sc, keys, n_max, d_n, bit_lo, bit_hi, vals_identity,
+                              have_hist, err);
 }
 
 } // namespace nbx

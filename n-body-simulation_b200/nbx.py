@@ -154,6 +154,7 @@ def lib() -> C.CDLL:
         "nbx_ensemble_sizes": [C.c_uint32, C.c_uint32, C.c_uint32, vp],
         "nbx_autotune": [vp, C.c_int, C.c_uint32, C.POINTER(Params),
                          C.POINTER(C.c_float)],
+        "nbx_accel_at": [vp, vp, vp, C.c_uint32, vp, vp],
         "nbx_direct_fp64_noalloc": [vp, vp, vp, C.c_uint32, vp, C.c_uint32,
                                     C.c_double, vp, vp, vp],
     }
@@ -449,6 +450,17 @@ class Handle:
         ax = np.zeros(len(t), np.float64)
         ay = np.zeros(len(t), np.float64)
         self._c(lib().nbx_direct_fp64(self.h, t, len(t), ax, ay))
+        return ax, ay
+
+    def accel_at(self, px, py):
+        """QuadTree::acceleration at arbitrary points from instance 0's last
+        tree with the handle's theta and epsilon."""
+        x = np.ascontiguousarray(px, np.float32)
+        y = np.ascontiguousarray(py, np.float32)
+        ax = np.zeros(len(x), np.float32)
+        ay = np.zeros(len(x), np.float32)
+        self._c(lib().nbx_accel_at(self.h, x.ctypes.data, y.ctypes.data, len(x),
+                                   ax.ctypes.data, ay.ctypes.data))
         return ax, ay
 
     def force_error(self, targets):

@@ -127,3 +127,43 @@ def test_cold_square_4m_build_bit_exact(nbx, oracle):
         assert same_bits(t[k], v), k
     assert np.array_equal(sim.download()["id"], sb["id"])
     sim.close()
+
+
+def collide_at_scale_cases(nbx):
+    # a compressed 1M cold square: most boxes overlap several neighbours
+    c = nbx.cold_square(1 << 20, 4)
+    c["px"] *= np.float32(0.35)
+    c["py"] *= np.float32(0.35)
+    yield "cold_dense_1M", c
+    # the headline two discs late in a run (contacts have piled up)
+    sim = nbx.Simulation(nbx.two_discs(1 << 20, 0, 0.2), theta=0.5)
+    sim.step(1000)
+    sim.phase("iterate")
+    yield "two_discs_1M_step1000", sim.download()
+    sim.close()
+    # the 4M cold square (its configuration's softening) 600 steps in
+    n = 1 << 22
+    sim = nbx.Simulation(nbx.cold_square(n, 0), theta=0.5, epsilon=1e-3 * 3.0 * np.sqrt(n))
+    sim.step(600)
+    sim.phase("iterate")
+    yield "cold_4M_step600", sim.download()
+    sim.close()
+
+
+def test_collisions_bit_exact_at_scale(nbx, oracle):
+    """Candidate pairs (set and pairLess order) and the resolved state bit
+    for bit against the oracle's sequential collide() on collision-heavy
+    states at the configurations' full sizes."""
+    for label, st in collide_at_scale_cases(nbx):
+        sim = nbx.Simulation(st)
+        sim.phase("collide")
+        gl, ge = sim.pairs()
+        pairs, depth = sim.collision_stats()
+        ol, oe = oracle.collision_pairs(st)
+        assert len(ol) > 100000, (label, len(ol))
+        assert pairs == len(ol), label
+        assert np.array_equal(gl, ol) and np.array_equal(ge, oe), label
+        out = sim.download()
+        ref, _ = oracle.collide(st)
+        assert same_bits(out, ref), (label, int((out != ref).sum()), depth)
+        sim.close()
