@@ -77,6 +77,12 @@ typedef struct nbx_params {
                              (src/naive/NaiveSimulation.cpp:17-57,
                              src/cuda/CudaNaive.cu:17-57); no tree is built,
                              use_mlp must be 0 */
+  int32_t force_block;    /* threads per block of the default force walk:
+                             128, 256 or 512 (0 = 256) */
+  int32_t leaf_pairs;     /* default force walk: 1 takes a leaf's bodies two
+                             at a time with paired FP32 instructions, 0 one
+                             at a time (default 1); the same terms either
+                             way, summed in another order */
 } nbx_params;
 
 typedef struct nbx_handle nbx_handle;
@@ -395,8 +401,10 @@ int nbx_mlp_eval(nbx_handle *h, const float *features, uint32_t n, float *out,
                  int tensor_cores);
 
 /* --- autotuner (no counterpart in the reference) ---
- * Times `steps` steps from the current state for each candidate -- force
- * launch grids {one warp per 32 bodies, 4, 8 or 16 blocks per SM} and, if
+ * Times `steps` steps from the current state for each candidate -- for the
+ * default plain walk the block shape (force_block 128, 256, 512 threads)
+ * and the leaf width (leaf_pairs 1 or 0); force launch grids {one warp per
+ * 32 bodies, 1/2, 1 or 2 SMs' worth of resident blocks per SM}; and, if
  * allow_leaf, leaf capacities {8, 12, 16, 24, 32} (a leaf capacity other
  * than 16 changes the tree, so results then differ from the reference's) --
  * keeps the fastest in the handle's parameters, and restores the state.

@@ -29,7 +29,8 @@ void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
 void launch_bfs_tree(cudaStream_t s, const DevState &S, ScanScratch &scan,
                      SortScratch &sort);
 void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
-                   const MlpDev *mlp, float band, int corr, bool noClamp);
+                   const MlpDev *mlp, float band, int corr, bool noClamp, int threads,
+                   bool pairs);
 void render_vertices(cudaStream_t s, const float4 *pv, const float2 *mr, uint32_t n,
                      const RenderParams &P, float4 *v0, float4 *v1, uint32_t *tiles,
                      double4 *partial, unsigned long long *total, float *stats);
@@ -507,7 +508,8 @@ DevState enqueue_step(nbx_handle *h, cudaStream_t s, DevState S) {
   if (h->timedCapture) cudaEventRecordWithFlags(h->forceMark[0], s, cudaEventRecordExternal);
   launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
                 h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
-                h->params.use_mlp, forces_unclamped(h));
+                h->params.use_mlp, forces_unclamped(h), h->params.force_block,
+                h->params.leaf_pairs != 0);
   if (h->timedCapture) cudaEventRecordWithFlags(h->forceMark[1], s, cudaEventRecordExternal);
   mark(s, "forces");
   return S;
@@ -634,7 +636,10 @@ bool valid_params(const nbx_params *p) {
   return p && p->dt == p->dt && p->theta >= 0.0f && p->epsilon >= 0.0f &&
          p->leaf_capacity >= 1 && p->leaf_capacity <= 64 && p->use_mlp >= 0 &&
          p->use_mlp <= 2 && (p->force_law == 0 || p->force_law == 1) &&
-         !(p->force_law == 1 && p->use_mlp != 0);
+         !(p->force_law == 1 && p->use_mlp != 0) &&
+         (p->force_block == 0 || p->force_block == 128 || p->force_block == 256 ||
+          p->force_block == 512) &&
+         (p->leaf_pairs == 0 || p->leaf_pairs == 1);
 }
 
 } // namespace
@@ -666,6 +671,8 @@ int nbx_params_default(nbx_params *p) {
   p->device = -1;
   p->mlp_band = 0.5f;
   p->force_law = 0;
+  p->force_block = 0;
+  p->leaf_pairs = 1;
   return NBX_OK;
 }
 
@@ -1302,7 +1309,8 @@ int nbx_phase(nbx_handle *h, int phase) {
     if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
     launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
                   h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
-                  h->params.use_mlp, forces_unclamped(h));
+                  h->params.use_mlp, forces_unclamped(h), h->params.force_block,
+                h->params.leaf_pairs != 0);
     break;
   case NBX_PHASE_ATTRACT:
     if (h->params.force_law == 1) {
@@ -1320,7 +1328,8 @@ int nbx_phase(nbx_handle *h, int phase) {
     h->forceInput = true;
     launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
                   h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
-                  h->params.use_mlp, forces_unclamped(h));
+                  h->params.use_mlp, forces_unclamped(h), h->params.force_block,
+                h->params.leaf_pairs != 0);
     break;
   case NBX_PHASE_STEP:
     enqueue_step(h, s, S);
@@ -1913,17 +1922,39 @@ int nbx_autotune(nbx_handle *h, int allowLeaf, uint32_t steps, nbx_params *best,
   if (allowLeaf) leaves = {8, 12, 16, 24, 32};
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
-  const int grids[] = {0, sms * 4, sms * 8, sms * 16};
+  // block shape and leaf width apply to the default plain walk only
+  const bool plain = !start.exact_math && start.use_mlp == 0;
+  std::vector<int> blockShapes = {start.force_block};
+  std::vector<int> leafWidths = {start.leaf_pairs};
+  if (plain) {
+    blockShapes = {128, 256, 512};
+    leafWidths = {1, 0};
+  }
+  struct Trial {
+    int leaf, threads, pairs, grid;
+  };
+  std::vector<Trial> trials;
+  for (int leaf : leaves)
+    for (int threads : blockShapes)
+      for (int pairs : leafWidths) {
+        // grids: one warp per 32 bodies, or a half, one or two full SMs'
+        // worth of resident blocks per SM
+        const int perSm = 2048 / (threads > 0 ? threads : 256);
+        for (int grid : {0, sms * perSm / 2, sms * perSm, sms * perSm * 2})
+          trials.push_back({leaf, threads, pairs, grid});
+      }
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   nbx_params bestP = start;
   float bestT = 1e30f;
-  for (int leaf : leaves) {
-    for (int grid : grids) {
+  {
+    for (const Trial &tr : trials) {
       nbx_params p = start;
-      p.leaf_capacity = leaf;
-      p.force_blocks = grid;
+      p.leaf_capacity = tr.leaf;
+      p.force_blocks = tr.grid;
+      p.force_block = tr.threads;
+      p.leaf_pairs = tr.pairs;
       h->params = p;
       sync_params(h);
       destroy_graphs(h);
@@ -1941,7 +1972,6 @@ int nbx_autotune(nbx_handle *h, int allowLeaf, uint32_t steps, nbx_params *best,
         bestP = p;
       }
     }
-    if (rc) break;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

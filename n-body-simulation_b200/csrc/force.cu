@@ -355,8 +355,9 @@ __device__ __forceinline__ void walk_plain_x2(const DevState &S, float tSq, floa
   ayOut = ay + (ly0 + ly1);
 }
 
-// Every target of the launch, one warp per 32.
-template <bool kExact, bool kCount, int kCorr, bool kClamp>
+// Every target of the launch, one warp per 32.  kPairs selects the paired
+// leaf loop for the default plain walk.
+template <bool kExact, bool kCount, int kCorr, bool kClamp, bool kPairs>
 __device__ __forceinline__ void forces_walk(
     const DevState &S, float tSq, float eSq, unsigned long long *counts,
     float bandSq, float eps, const float2 *__restrict__ query, uint32_t nQuery,
@@ -392,7 +393,7 @@ __device__ __forceinline__ void forces_walk(
     uint32_t nFar = 0, nNear = 0, nVisit = 0, nIter = 0, nChunk = 0;
     // the clamp-free law only while no lane's instance reaches beyond the
     // coordinate limit (the build's per-instance flag)
-    constexpr bool kPlainX2 = !kExact && !kCount && kCorr == 0 && !kClamp;
+    constexpr bool kPlainX2 = kPairs && !kExact && !kCount && kCorr == 0 && !kClamp;
     const bool anyWide = !kClamp && __any_sync(0xffffffffu, wide);
     if (anyWide)
       walk_targets<kExact, kCount, kCorr, true>(S, tSq, eSq, bandSq, eps, x, y, cur,
@@ -434,18 +435,22 @@ __device__ __forceinline__ void forces_walk(
 // which the host picks only for non-negative masses below its bound; a
 // warp holding a target whose instance reaches beyond the coordinate limit
 // stored at upload (the build's SegDev::wide), where distances could
-// overflow, takes the clamped walk instead.  Launch bounds: 8 blocks of 256
-// threads per SM (at most 32 registers, none spilled) for every walk but the
-// learned correction's, whose MMA fragments keep it at 3.
-template <bool kExact, bool kCount = false, int kCorr = 0, bool kClamp = true>
-__global__ void __launch_bounds__(kForceBlock, kCorr == 1 ? 3 : 8)
+// overflow, takes the clamped walk instead.  Launch bounds: a full SM of
+// kBlock-thread blocks (2048 threads: at most 32 registers) for every walk
+// but the learned correction's, whose MMA fragments keep it at 3 blocks of
+// 256.  kBlock and kPairs vary only for the default plain walk (the
+// autotuner's block shape and leaf width).
+template <bool kExact, bool kCount = false, int kCorr = 0, bool kClamp = true,
+          int kBlock = kForceBlock, bool kPairs = true>
+__global__ void __launch_bounds__(kBlock, kCorr == 1 ? 3 : 2048 / kBlock)
     k_forces(DevState S, float tSq, float eSq,
              unsigned long long *counts = nullptr,
              const MlpDev *__restrict__ mlp = nullptr, float bandSq = 0.0f,
              float eps = 0.0f, const float2 *__restrict__ query = nullptr,
              uint32_t nQuery = 0, float2 *__restrict__ queryAcc = nullptr) {
-  constexpr int kStage = kCorr == 1 ? kWarps : 1;
-  __shared__ float4 sBody[kWarps][32];
+  constexpr int kBlockWarps = kBlock / 32;
+  constexpr int kStage = kCorr == 1 ? kBlockWarps : 1;
+  __shared__ float4 sBody[kBlockWarps][32];
   __shared__ MlpDev sW;
   __shared__ __nv_bfloat16 sStage[kStage][32][16];
   if (kCorr == 1) {
@@ -453,8 +458,8 @@ __global__ void __launch_bounds__(kForceBlock, kCorr == 1 ? 3 : 8)
       reinterpret_cast<uint32_t *>(&sW)[q] = reinterpret_cast<const uint32_t *>(mlp)[q];
     __syncthreads();
   }
-  forces_walk<kExact, kCount, kCorr, kClamp>(S, tSq, eSq, counts, bandSq, eps, query, nQuery,
-                                             queryAcc, sBody, sW, sStage);
+  forces_walk<kExact, kCount, kCorr, kClamp, kPairs>(S, tSq, eSq, counts, bandSq, eps, query,
+                                                     nQuery, queryAcc, sBody, sW, sStage);
 }
 
 // FMA throughput probe: 8 independent chains per thread.
@@ -524,8 +529,30 @@ void launch_query_forces(cudaStream_t s, const DevState &S, bool exact,
                                                       nq, out);
 }
 
+// The default plain walk with kBlock threads per block and the paired or
+// single-body leaf loop.
+template <int kBlock>
+void launch_plain(cudaStream_t s, const DevState &S, int blocks, bool pairs) {
+  if (blocks <= 0) {
+    const uint32_t warps = (S.n + 31) / 32, per = kBlock / 32;
+    const uint32_t b = (warps + per - 1) / per;
+    blocks = (int)(b ? b : 1);
+  }
+  if (pairs)
+    k_forces<false, false, 0, false, kBlock, true><<<blocks, kBlock, 0, s>>>(S, S.tSq, S.eSq);
+  else
+    k_forces<false, false, 0, false, kBlock, false><<<blocks, kBlock, 0, s>>>(S, S.tSq, S.eSq);
+}
+
 void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
-                   const MlpDev *mlp, float band, int corr, bool noClamp) {
+                   const MlpDev *mlp, float band, int corr, bool noClamp, int threads,
+                   bool pairs) {
+  if (corr == 0 && !exact && noClamp) {
+    if (threads == 128) launch_plain<128>(s, S, blocks, pairs);
+    else if (threads == 512) launch_plain<512>(s, S, blocks, pairs);
+    else launch_plain<256>(s, S, blocks, pairs);
+    return;
+  }
   if (blocks <= 0) {
     uint32_t warps = (S.n + 31) / 32;
     uint32_t b = (warps + kWarps - 1) / kWarps;
@@ -542,8 +569,6 @@ void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
         S, S.tSq, S.eSq, nullptr, nullptr, band * band, sqrtf(S.eSq));
   else if (exact)
     k_forces<true><<<blocks, kForceBlock, 0, s>>>(S, S.tSq, S.eSq);
-  else if (noClamp)
-    k_forces<false, false, 0, false><<<blocks, kForceBlock, 0, s>>>(S, S.tSq, S.eSq);
   else
     k_forces<false><<<blocks, kForceBlock, 0, s>>>(S, S.tSq, S.eSq);
 }

@@ -60,7 +60,8 @@ class Params(C.Structure):
                 ("exact_math", C.c_int32), ("use_mlp", C.c_int32),
                 ("node_factor", C.c_float), ("pair_factor", C.c_float),
                 ("force_blocks", C.c_int32), ("device", C.c_int32),
-                ("mlp_band", C.c_float), ("force_law", C.c_int32)]
+                ("mlp_band", C.c_float), ("force_law", C.c_int32),
+                ("force_block", C.c_int32), ("leaf_pairs", C.c_int32)]
 
 
 class Camera(C.Structure):
@@ -524,6 +525,7 @@ class Handle:
         self._c(lib().nbx_autotune(self.h, int(allow_leaf), steps, C.byref(p),
                                    C.byref(ms)))
         return {"leaf_capacity": p.leaf_capacity, "force_blocks": p.force_blocks,
+                "force_block": p.force_block, "leaf_pairs": p.leaf_pairs,
                 "ms_per_step": ms.value}
 
     # -- learned far-field correction --------------------------------

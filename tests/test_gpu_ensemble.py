@@ -80,12 +80,39 @@ def test_autotune_restores_state(nbx):
     before = h.download()
     best = h.autotune(allow_leaf=False, steps=2)
     assert best["leaf_capacity"] == 16 and best["ms_per_step"] > 0
+    # all three axes reported: grid, block shape, leaf width
+    assert best["force_block"] in (128, 256, 512) and best["leaf_pairs"] in (0, 1)
     assert same_bits(h.download(), before)
-    # stepping with the tuned launch gives the reference results
+    # stepping with the tuned launch equals a fresh handle with the same
+    # parameters bit for bit (grid and block shape change nothing; the leaf
+    # width only the summation order, checked against the default below)
     h.step(3)
-    ref = nbx.Handle(sizes, theta=0.5)
+    ref = nbx.Handle(sizes, theta=0.5, force_blocks=best["force_blocks"],
+                     force_block=best["force_block"], leaf_pairs=best["leaf_pairs"])
     ref.upload(bodies)
     ref.step(5)
     assert same_bits(h.download(), ref.download())
     h.close()
     ref.close()
+
+
+@pytest.mark.parametrize("threads", [128, 256, 512])
+@pytest.mark.parametrize("pairs", [0, 1])
+def test_plain_walk_shapes(nbx, oracle, threads, pairs):
+    """Every block shape and leaf width of the default walk against the
+    reference traversal (the bars of the default arithmetic), and block
+    shapes bit-identical to each other at one leaf width."""
+    from conftest import rel_err
+    b = nbx.uniform_disc(20000)
+    _, _, _, sb, tree = oracle.morton_build(b)
+    ox, oy = oracle.tree_forces(sb["px"], sb["py"], sb["mass"], tree, 0.5, 1.0)
+    sim = nbx.Simulation(b, theta=0.5, force_block=threads, leaf_pairs=pairs)
+    sim.phase("attract")
+    g = sim.download()
+    e = rel_err(g["ax"], g["ay"], ox, oy)
+    assert np.percentile(e, 99) < 1e-5 and e.max() < 1e-4, (np.percentile(e, 99), e.max())
+    base = nbx.Simulation(b, theta=0.5, force_block=256, leaf_pairs=pairs)
+    base.phase("attract")
+    assert same_bits(g, base.download())
+    sim.close()
+    base.close()
