@@ -128,7 +128,9 @@ void exclusive_scan_u32(cudaStream_t s, const uint32_t *in, uint32_t *out,
   const uint32_t tiles = (n_max + kScanTile - 1) / kScanTile;
   uint32_t *tileSum = reinterpret_cast<uint32_t *>(sc.status);
   (void)err;
-  k_scan_reduce<<<tiles > 0 ? tiles : 1, kScanThreads, 0, s>>>(in, n_max, d_n, tileSum);
+  // a single tile adds no earlier tile sums: no reduce pass
+  if (tiles > 1)
+    k_scan_reduce<<<tiles, kScanThreads, 0, s>>>(in, n_max, d_n, tileSum);
   k_scan_apply<<<tiles > 0 ? tiles : 1, kScanThreads, 0, s>>>(in, out, n_max, d_n, total,
                                                                tileSum);
 }
