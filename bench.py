@@ -232,8 +232,8 @@ def forms_leg(nbx, torch, sim, n, local, ids, args):
     {0.5, 0.7, 0.9, 1.1} (plus the points nearest plain theta 0.5's cost):
     body-steps/s and the force error against the FP64 direct sum on the
     same 4096 sampled bodies.  Also the error floor of the reference's law
-    itself: theta 0 (every body summed with fastInvSqrt, no cells) on 1024 of
-    those bodies."""
+    itself (fastInvSqrt against the exact law, FP64 sums over every body) on
+    1024 of those bodies."""
     state = sim.download()
     pos = np.empty(n, np.int64)
     pos[state["id"]] = np.arange(n)
@@ -261,19 +261,13 @@ def forms_leg(nbx, torch, sim, n, local, ids, args):
                     "body_steps_per_s": n / (ms * 1e-3), "ms_per_step": ms,
                     "p50": err["median"], "p99": err["p99"], "steps": steps})
         h.close()
-    # the law's own floor: theta 0 sums every body (with the reference's
-    # fastInvSqrt); against the FP64 law
+    # the floor under every form: the reference's fastInvSqrt law against
+    # the exact law, both summed over every body in FP64
     h = nbx.Simulation(state, theta=0.5, device=local)
-    h.phase("build")
-    h.set_params(theta=0.0)
-    t0 = tg[:1024]
-    ax, ay = h.accel_at(state["px"][t0], state["py"][t0])
-    ex, ey = h.direct_fp64(t0)
+    fl = h.law_error(tg[:1024])
     h.close()
-    e = np.hypot(ax - ex, ay - ey) / np.hypot(ex, ey)
-    floor = {"form": "law floor (theta 0: fastInvSqrt law against the FP64 law)",
-             "samples": 1024, "p50": float(np.median(e)),
-             "p99": float(np.percentile(e, 99)), "max": float(e.max())}
+    floor = {"form": "law floor: fastInvSqrt law vs exact law, both FP64 all-body sums",
+             "samples": 1024, "p50": fl["median"], "p99": fl["p99"], "max": fl["max"]}
     return {"forms": out, "law_floor": floor}
 
 

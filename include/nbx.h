@@ -312,6 +312,17 @@ int nbx_direct_fp64_noalloc(const float *x, const float *y, const float *mass,
 int nbx_force_error_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m,
                          double *stats, double *err);
 
+/* Error of the reference's force law itself: for the given targets, the
+ * relative difference between the FP64 direct sum of the tree law computed
+ * with the reference's fastInvSqrt (QuadTree.cpp:11-26, applied to the
+ * float distance squared) and the FP64 direct sum of the exact law;
+ * stats = {median, p99, max, mean}.  No tree and no float summation enter,
+ * so this is the floor under the force error of every form that keeps the
+ * reference's law.  Tree law (force_law 0) only.  No counterpart in the
+ * reference. */
+int nbx_law_error_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m,
+                       double *stats);
+
 /* Compensated FP64 sums over all bodies: {kinetic energy, px, py, Lz,
  * total mass}.  No counterpart in the reference. */
 int nbx_energy_momentum_fp64(nbx_handle *h, double *out5);

@@ -1549,6 +1549,36 @@ int nbx_direct_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m, double *
   return direct_sums(h, targets, m, h->params.force_law == 1 ? 1 : 0, ax, ay);
 }
 
+int nbx_law_error_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m,
+                       double *stats) {
+  if (!h || !stats || (m && !targets)) return NBX_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (h->params.force_law != 0) return fail(h, NBX_ERR_STATE, "defined for the tree law");
+  for (int k = 0; k < 4; ++k) stats[k] = 0.0;
+  if (m == 0) return NBX_OK;
+  for (uint32_t k = 0; k < m; ++k)
+    if (targets[k] >= h->n) return fail(h, NBX_ERR_ARG, "target index out of range");
+  std::vector<double> ex(m), ey(m), fx(m), fy(m);
+  int rc = direct_sums(h, targets, m, 0, ex.data(), ey.data());
+  if (rc) return rc;
+  rc = direct_sums(h, targets, m, 4, fx.data(), fy.data());
+  if (rc) return rc;
+  std::vector<double> e(m);
+  double mean = 0.0;
+  for (uint32_t k = 0; k < m; ++k) {
+    const double dx = fx[k] - ex[k], dy = fy[k] - ey[k];
+    e[k] = std::sqrt(dx * dx + dy * dy) /
+           std::max(std::sqrt(ex[k] * ex[k] + ey[k] * ey[k]), 1e-30);
+    mean += e[k];
+  }
+  std::sort(e.begin(), e.end());
+  stats[0] = e[m / 2];
+  stats[1] = e[std::min<size_t>(m - 1, (size_t)(0.99 * m))];
+  stats[2] = e.back();
+  stats[3] = mean / m;
+  return NBX_OK;
+}
+
 int nbx_potential_fp64(nbx_handle *h, const uint32_t *targets, uint32_t m, double *phi,
                        double *u) {
   if (!h || !u || (targets && m && !phi)) return NBX_ERR_ARG;

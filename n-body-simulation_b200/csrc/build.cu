@@ -496,22 +496,51 @@ __global__ void __launch_bounds__(kBlock) k_upward(DevState S) {
 // only when asked for (launch_bfs_tree).
 
 // Nodes starting at each body (splitCount) and the depth of the first one
-// (splitLo).
+// (splitLo).  hi_j = min(lcp(j, j+L), 31) (-1 when j+L leaves the
+// instance) is formed once per body into shared memory, then each body
+// takes the maximum over its L+1 windows.
+constexpr int kMaxLeafCap = 64; // nbx_params leaf_capacity bound
 __global__ void __launch_bounds__(kBlock) k_trav_counts(DevState S) {
+  __shared__ int8_t sHi[kBlock + kMaxLeafCap];
   const uint64_t *c = S.sortedCodes;
   const uint32_t L = (uint32_t)S.leafCapacity;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n;
-       i += gridDim.x * blockDim.x) {
+  for (uint32_t b0 = blockIdx.x * kBlock; b0 < S.n; b0 += gridDim.x * kBlock) {
+    // windows j in [b0 - L, b0 + kBlock)
+    const uint32_t jBase = b0 >= L ? b0 - L : 0u;
+    const uint32_t span = b0 + kBlock - jBase;
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < span; t += kBlock) {
+      const uint32_t j = jBase + t;
+      int hi = -1;
+      if (j < S.n) {
+        const SegDev &G = S.seg[S.segOf[j]];
+        if ((uint64_t)j + L < (uint64_t)G.start + G.count)
+          hi = min(lcp_digits(c[j], c[j + L]), kMaxDepth - 1);
+      }
+      sHi[t] = (int8_t)hi;
+    }
+    __syncthreads();
+    const uint32_t i = b0 + threadIdx.x;
+    if (i >= S.n) continue;
     const SegDev &G = S.seg[S.segOf[i]];
-    const uint32_t s0 = G.start, s1 = G.start + G.count;
-    const uint64_t ci = c[i];
-    const int lo = (i == s0) ? 0 : lcp_digits(c[i - 1], ci) + 1;
+    const uint32_t s0 = G.start;
+    const int lo = (i == s0) ? 0 : lcp_digits(c[i - 1], c[i]) + 1;
     int w = -1;
-    for (uint32_t j = i >= s0 + L ? i - L : s0; j <= i && (uint64_t)j + L < s1; ++j)
-      w = max(w, min(lcp_digits(c[j], c[j + L]), kMaxDepth - 1));
+    for (uint32_t j = i >= s0 + L ? i - L : s0; j <= i; ++j) w = max(w, (int)sHi[j - jBase]);
     const int leaf = w + 1;
     S.splitCount[i] = lo <= leaf ? (uint32_t)(leaf - lo + 1) : 0u;
     S.splitLo[i] = (uint8_t)lo; // <= 33
+  }
+}
+
+// Record -> first body: body i owns records P_i .. P_i + count_i - 1.
+__global__ void __launch_bounds__(kBlock) k_trav_owner(DevState S, uint32_t *owner) {
+  const uint32_t total = S.counters[6];
+  if (total > S.nodeCapacity) return;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t cnt = S.splitCount[i], P = S.splitStart[i];
+    for (uint32_t k = 0; k < cnt; ++k) owner[P + k] = i;
   }
 }
 
@@ -565,76 +594,86 @@ __device__ __forceinline__ uint32_t prefix_start(const uint64_t *c, uint32_t s0,
   return lo;
 }
 
-// The records of every node: body range, next and open slots, size and
-// centre (splitNode's arithmetic along the path), parent and number of
-// non-empty children; arrival counters cleared.
-__global__ void __launch_bounds__(kBlock) k_trav_nodes(DevState S) {
+// Record of the node at depth d starting at body b.
+__device__ __forceinline__ uint32_t record_of(const DevState &S, uint32_t b, int d) {
+  return S.splitStart[b] + (uint32_t)(d - (int)S.splitLo[b]);
+}
+
+// One thread per record: body range, next and open slots, size and centre
+// (splitNode's arithmetic along the path), parent, the records of the
+// non-empty children in digit order (all ones past the last); arrival
+// counters cleared.
+__global__ void __launch_bounds__(kBlock)
+    k_trav_nodes(DevState S, const uint32_t *__restrict__ owner, uint4 *__restrict__ kids) {
   const uint64_t *c = S.sortedCodes;
   const uint32_t total = S.counters[6];
   const bool overflow = total > S.nodeCapacity;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n;
-       i += gridDim.x * blockDim.x) {
-    const uint32_t sg = S.segOf[i];
-    SegDev &G = S.seg[sg];
-    const uint32_t s0 = G.start, s1 = G.start + G.count;
-    const uint32_t P = S.splitStart[i];
-    if (i == s0) {
-      // all-or-nothing: no instance gets a traversal, the step reports it
+  if (blockIdx.x == 0) {
+    // instance bases: all-or-nothing on overflow (the step reports it)
+    for (uint32_t sg = threadIdx.x; sg < S.nseg; sg += blockDim.x) {
+      SegDev &G = S.seg[sg];
+      if (G.count == 0) continue;
+      const uint32_t s0 = G.start, s1 = G.start + G.count;
+      const uint32_t P = S.splitStart[s0];
       G.travBase = overflow ? 0u : P;
       G.travCount = overflow ? 0u : (s1 < S.n ? S.splitStart[s1] : total) - P;
-      if (overflow && sg == 0) atomicOr(S.status, kStatusTreeCapacity);
     }
-    const uint32_t cnt = S.splitCount[i];
-    if (overflow || cnt == 0) continue;
+    if (overflow && threadIdx.x == 0) atomicOr(S.status, kStatusTreeCapacity);
+  }
+  if (overflow) return;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total;
+       p += gridDim.x * blockDim.x) {
+    const uint32_t i = owner[p];
+    const SegDev &G = S.seg[S.segOf[i]];
+    const uint32_t s0 = G.start, s1 = G.start + G.count;
+    const uint32_t P = S.splitStart[i];
+    const uint32_t k = p - P;
     const int lo = S.splitLo[i];
+    const int d = lo + (int)k;
+    const bool leaf = k + 1 == S.splitCount[i];
     const uint64_t ci = c[i];
     float cx = G.cx, cy = G.cy, size = G.size;
-    for (int t = 0; t < lo; ++t) {
+    for (int t = 0; t < d; ++t) {
       size = __fmul_rn(size, 0.5f);
       const int q = digit_at(ci, t);
       cx = __fadd_rn(cx, __fmul_rn((float)(q & 1) - 0.5f, size));
       cy = __fadd_rn(cy, __fmul_rn((float)(q >> 1) - 0.5f, size));
     }
-    uint32_t e = s1; // ends shrink with depth
-    for (uint32_t k = 0; k < cnt; ++k) {
-      const int d = lo + (int)k;
+    const uint32_t e = d > 0 ? prefix_end(c, i, s1, d, ci >> (64 - 2 * d)) : s1;
+    // the record after the subtree; all ones past the instance's last
+    const uint32_t next = e < s1 ? S.splitStart[e] : 0xffffffffu;
+    int32_t parent = -1;
+    if (d > 0) {
       if (k > 0) {
-        size = __fmul_rn(size, 0.5f);
-        const int q = digit_at(ci, d - 1);
-        cx = __fadd_rn(cx, __fmul_rn((float)(q & 1) - 0.5f, size));
-        cy = __fadd_rn(cy, __fmul_rn((float)(q >> 1) - 0.5f, size));
+        parent = (int32_t)(p - 1);
+      } else {
+        // the depth-(d-1) node around i starts before it (the root at s0)
+        const uint32_t j = d == 1 ? s0 : prefix_start(c, s0, i, d - 1);
+        parent = (int32_t)record_of(S, j, d - 1);
       }
-      const uint32_t p = P + k;
-      const bool leaf = k + 1 == cnt;
-      if (d > 0) e = prefix_end(c, i, e, d, ci >> (64 - 2 * d));
-      // the record after the subtree; all ones past the instance's last
-      const uint32_t next = e < s1 ? S.splitStart[e] : 0xffffffffu;
-      int32_t parent = -1;
-      if (d > 0) {
-        if (k > 0) {
-          parent = (int32_t)(p - 1);
-        } else {
-          // the depth-(d-1) node around i starts before it (the root at s0)
-          const uint32_t j = d == 1 ? s0 : prefix_start(c, s0, i, d - 1);
-          parent = (int32_t)(S.splitStart[j] + (uint32_t)(d - 1 - (int)S.splitLo[j]));
-        }
-      }
-      uint32_t children = 0;
-      if (!leaf) {
-        const uint32_t b1 = first_with_digit(c, i, e, d, 1);
-        const uint32_t b2 = first_with_digit(c, b1, e, d, 2);
-        const uint32_t b3 = first_with_digit(c, b2, e, d, 3);
-        children = (b1 > i) + (b2 > b1) + (b3 > b2) + (e > b3);
-      }
-      TravNode &T = S.tN[p];
-      T.a = make_float4(0.0f, 0.0f, 0.0f, __fmul_rn(size, size));
-      T.b = make_int4((int)next, (int)(leaf ? next : p + 1), (int)i, (int)e);
-      S.tM[p] = make_float4(0.0f, 0.0f, 0.0f, size);
-      S.tC[p] = make_float2(cx, cy);
-      S.parent[p] = parent;
-      S.subtree[p] = children;
-      S.arrive[p] = 0u;
     }
+    uint4 ch = make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu);
+    uint32_t children = 0;
+    if (!leaf) {
+      uint32_t bound[5];
+      bound[0] = i;
+      bound[4] = e;
+      for (int q = 1; q < 4; ++q) bound[q] = first_with_digit(c, bound[q - 1], e, d, q);
+      uint32_t r[4];
+      for (int q = 0; q < 4; ++q)
+        if (bound[q + 1] > bound[q]) r[children++] = record_of(S, bound[q], d + 1);
+      for (uint32_t q = children; q < 4; ++q) r[q] = 0xffffffffu;
+      ch = make_uint4(r[0], r[1], r[2], r[3]);
+    }
+    TravNode &T = S.tN[p];
+    T.a = make_float4(0.0f, 0.0f, 0.0f, __fmul_rn(size, size));
+    T.b = make_int4((int)next, (int)(leaf ? next : p + 1), (int)i, (int)e);
+    S.tM[p] = make_float4(0.0f, 0.0f, 0.0f, size);
+    S.tC[p] = make_float2(cx, cy);
+    S.parent[p] = parent;
+    S.subtree[p] = children;
+    S.arrive[p] = 0u;
+    kids[p] = ch;
   }
 }
 
@@ -642,13 +681,14 @@ __global__ void __launch_bounds__(kBlock) k_trav_nodes(DevState S) {
 // (sumNode's order) and climbs; the last non-empty child to arrive sums its
 // parent's children in digit order, then finishNode's divide; second
 // moments about each centre of mass for the corrected forms.
-__global__ void __launch_bounds__(kBlock) k_trav_upward(DevState S) {
+__global__ void __launch_bounds__(kBlock)
+    k_trav_upward(DevState S, const uint4 *__restrict__ kids) {
   const uint32_t total = S.counters[6];
   if (total > S.nodeCapacity) return;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total;
        p += gridDim.x * blockDim.x) {
+    if (S.subtree[p] != 0) continue; // interior: summed by its last child
     const int4 B = S.tN[p].b;
-    if (B.y != B.x) continue; // interior: summed by its last child
     const uint32_t b0 = (uint32_t)B.z, b1 = min((uint32_t)B.w, S.n);
     float px = 0.0f, py = 0.0f, mm = 0.0f;
     for (uint32_t b = b0; b < b1; ++b) {
@@ -687,28 +727,33 @@ __global__ void __launch_bounds__(kBlock) k_trav_upward(DevState S) {
                    : "l"(&S.arrive[g])
                    : "memory");
       if (old + 1 != children) break;
+      const uint4 kv = kids[g];
+      const uint32_t r[4] = {kv.x, kv.y, kv.z, kv.w};
+      float cxs[4], cys[4];
+      float4 ca[4], mo[4];
+      for (uint32_t q = 0; q < 4; ++q) {
+        if (q >= children || r[q] >= total) continue;
+        cxs[q] = __ldcg(&S.sumX[r[q]]);
+        cys[q] = __ldcg(&S.sumY[r[q]]);
+        ca[q] = __ldcg(&S.tN[r[q]].a);
+        mo[q] = __ldcg(&S.tM[r[q]]);
+      }
       float sx = 0.0f, sy = 0.0f, sm = 0.0f;
-      uint32_t ch = g + 1;
-      for (uint32_t q = 0; q < children && ch < total; ++q) {
-        const float cxs = __ldcg(&S.sumX[ch]), cys = __ldcg(&S.sumY[ch]);
-        const float cm = __ldcg(&S.tN[ch].a.z);
-        sx = q == 0 ? cxs : __fadd_rn(sx, cxs);
-        sy = q == 0 ? cys : __fadd_rn(sy, cys);
-        sm = q == 0 ? cm : __fadd_rn(sm, cm);
-        ch = (uint32_t)S.tN[ch].b.x;
+      for (uint32_t q = 0; q < children && q < 4; ++q) {
+        if (r[q] >= total) break;
+        sx = q == 0 ? cxs[q] : __fadd_rn(sx, cxs[q]);
+        sy = q == 0 ? cys[q] : __fadd_rn(sy, cys[q]);
+        sm = q == 0 ? ca[q].z : __fadd_rn(sm, ca[q].z);
       }
       const float dv = fmaxf(sm, FLT_MIN);
       const float PX = __fdiv_rn(sx, dv), PY = __fdiv_rn(sy, dv);
       float jxx = 0.0f, jyy = 0.0f, jxy = 0.0f;
-      ch = g + 1;
-      for (uint32_t q = 0; q < children && ch < total; ++q) {
-        const float4 a = __ldcg(&S.tN[ch].a);
-        const float4 mo = __ldcg(&S.tM[ch]);
-        const float dx = a.x - PX, dy = a.y - PY;
-        jxx += mo.x + a.z * dx * dx;
-        jyy += mo.y + a.z * dy * dy;
-        jxy += mo.z + a.z * dx * dy;
-        ch = (uint32_t)S.tN[ch].b.x;
+      for (uint32_t q = 0; q < children && q < 4; ++q) {
+        if (r[q] >= total) break;
+        const float dx = ca[q].x - PX, dy = ca[q].y - PY;
+        jxx += mo[q].x + ca[q].z * dx * dx;
+        jyy += mo[q].y + ca[q].z * dy * dy;
+        jxy += mo[q].z + ca[q].z * dx * dy;
       }
       __stcg(&S.sumX[g], sx);
       __stcg(&S.sumY[g], sy);
@@ -774,9 +819,13 @@ void launch_trav_tree(cudaStream_t s, const DevState &S, ScanScratch &scan) {
   exclusive_scan_u32(s, S.splitCount, S.splitStart, n, nullptr, &S.counters[6],
                      scan, S.status);
   mark(s, "tree.counts");
-  k_trav_nodes<<<grid_for(n), kBlock, 0, s>>>(S);
+  // per-record scratch in arrays only the breadth-first build uses
+  uint32_t *owner = reinterpret_cast<uint32_t *>(S.start);
+  uint4 *kids = reinterpret_cast<uint4 *>(S.moments);
+  k_trav_owner<<<grid_for(n), kBlock, 0, s>>>(S, owner);
+  k_trav_nodes<<<grid_for(n / 2 + 64), kBlock, 0, s>>>(S, owner, kids);
   mark(s, "tree.nodes");
-  k_trav_upward<<<grid_for(n / 4 + 64), kBlock, 0, s>>>(S);
+  k_trav_upward<<<grid_for(n / 4 + 64), kBlock, 0, s>>>(S, kids);
   mark(s, "tree.upward");
 }
 

@@ -15,8 +15,12 @@ constexpr int kDirectChunks = 64;
 // or the potential of either (per unit target mass): the tree law's is
 // -(m / eps) atan(eps / |d|) (its gradient is the tree force; -m / |d| for
 // eps = 0), the Plummer law's -m / sqrt(d^2 + eps^2).
+// kFastLawForce is the tree force law with the reference's fastInvSqrt
+// (QuadTree.cpp:11-26) applied to the float distance squared, accumulated in
+// FP64: the error of the reference's law itself, without any summation or
+// tree error.
 enum DirectKind { kTreeForce = 0, kPlummerForce = 1, kTreePotential = 2,
-                  kPlummerPotential = 3 };
+                  kPlummerPotential = 3, kFastLawForce = 4 };
 
 // Partial FP64 sums: block (tb, chunk) adds sources of `chunk` for the
 // targets tb*128 .. tb*128+127.  Sources staged through shared memory.
@@ -62,7 +66,11 @@ __global__ void __launch_bounds__(kDirectThreads)
         const double dSq = dx * dx + dy * dy;
         if (dSq == 0.0) continue;
         const double q = dSq + eSq;
-        if (kind == kTreeForce || kind == kPlummerForce) {
+        if (kind == kFastLawForce) {
+          const double f = (double)s.z * (double)fast_inv_sqrt((float)dSq) / (dSq + eSq);
+          ax += dx * f;
+          ay += dy * f;
+        } else if (kind == kTreeForce || kind == kPlummerForce) {
           const double f = kind == kPlummerForce ? (double)s.z / (q * sqrt(q))
                                                  : (double)s.z / (sqrt(dSq) * q);
           ax += dx * f;
@@ -155,7 +163,7 @@ __global__ void k_energy_final(const double *__restrict__ part, int blocks,
 
 // partial must hold kDirectChunks * m double2.
 // kind: 0 tree-law force, 1 Plummer force, 2 tree-law potential (to ax),
-// 3 Plummer potential (to ax).
+// 3 Plummer potential (to ax), 4 tree-law force with fastInvSqrt.
 void launch_direct_fp64(cudaStream_t s, const float4 *pv, const float2 *mr,
                         uint32_t n, const uint32_t *targets, const uint2 *ranges,
                         uint32_t m, double eps, int kind, double2 *partial,

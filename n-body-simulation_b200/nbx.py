@@ -41,7 +41,7 @@ EXPORTS = (
     "nbx_set_attractor", "nbx_reset", "nbx_nbs2_record", "nbx_nbs2_flush",
     "nbx_nbs2_open", "nbx_nbs2_write_packed", "nbx_nbs2_close",
     "nbx_draw_default", "nbx_render", "nbx_body_stats", "nbx_debug_expire_wait",
-    "nbx_potential_fp64", "nbx_collision_stats",
+    "nbx_potential_fp64", "nbx_collision_stats", "nbx_law_error_fp64",
 )
 SCENARIOS = {"disc": 0, "two_galaxies": 1, "cold_square": 2}
 MLP_PARAMS = 1442
@@ -132,6 +132,7 @@ def lib() -> C.CDLL:
         "nbx_energy_momentum_fp64": [vp, f64p],
         "nbx_potential_fp64": [vp, vp, C.c_uint32, vp, C.POINTER(C.c_double)],
         "nbx_collision_stats": [vp, C.POINTER(C.c_int64), C.POINTER(C.c_uint32)],
+        "nbx_law_error_fp64": [vp, u32p, C.c_uint32, f64p],
         "nbx_status_bits": [vp, C.POINTER(C.c_uint32)],
         "nbx_last_error": [vp],
         "nbx_uniform_disc": [C.c_uint32, C.c_uint32, bodyp],
@@ -452,6 +453,14 @@ class Handle:
         ay = np.zeros(len(t), np.float64)
         self._c(lib().nbx_direct_fp64(self.h, t, len(t), ax, ay))
         return ax, ay
+
+    def law_error(self, targets):
+        """Error of the reference's fastInvSqrt law against the exact law,
+        both summed in FP64 over every body, at the given targets."""
+        t = np.ascontiguousarray(targets, np.uint32)
+        st = np.zeros(4, np.float64)
+        self._c(lib().nbx_law_error_fp64(self.h, t, len(t), st))
+        return {"median": st[0], "p99": st[1], "max": st[2], "mean": st[3]}
 
     def accel_at(self, px, py):
         """QuadTree::acceleration at arbitrary points from instance 0's last

@@ -502,3 +502,35 @@ def test_force_clamp_guard_wide_frame(nbx, oracle, case):
     sim.close()
     assert np.array_equal(g["ax"], ox, equal_nan=True)
     assert np.array_equal(g["ay"], oy, equal_nan=True)
+
+
+def test_law_error_floor(nbx):
+    """The reference's fastInvSqrt law against the exact law, both summed in
+    FP64 over every body: the GPU's figure against a numpy evaluation of the
+    same two sums (test-side restatement)."""
+    s = nbx.uniform_disc(3000)
+    sim = nbx.Simulation(s)
+    tg = np.arange(0, 3000, 7, dtype=np.uint32)
+    got = sim.law_error(tg)
+    x = s["px"].astype(np.float64)
+    y = s["py"].astype(np.float64)
+    m = s["mass"].astype(np.float64)
+    errs = []
+    for t in tg:
+        dx, dy = x - x[t], y - y[t]
+        d2 = dx * dx + dy * dy
+        d2[t] = 1.0
+        v = d2.astype(np.float32)
+        g = (np.uint32(0x5f3759df) - (v.view(np.uint32) >> np.uint32(1))).view(np.float32)
+        fis = (g * (np.float32(1.5) - np.float32(0.5) * v * g * g)).astype(np.float64)
+        fe = m / (np.sqrt(d2) * (d2 + 1.0))
+        ff = m * fis / (d2 + 1.0)
+        fe[t] = ff[t] = 0.0
+        ex, ey = np.sum(dx * fe), np.sum(dy * fe)
+        fx, fy = np.sum(dx * ff), np.sum(dy * ff)
+        errs.append(np.hypot(fx - ex, fy - ey) / np.hypot(ex, ey))
+    errs = np.sort(errs)
+    assert abs(got["median"] - errs[len(errs) // 2]) < 1e-6 * errs[len(errs) // 2] + 1e-9
+    assert abs(got["max"] - errs[-1]) < 1e-5 * errs[-1]
+    assert 1e-4 < got["median"] < 2e-3  # the bit hack's one Newton step
+    sim.close()
