@@ -372,8 +372,6 @@ int allocate(nbx_handle *h) {
   A(S.largePairs, n + 64);
   A(S.fillLarge, n);
   A(S.nLater, n);
-  A(S.unitFlag, n);
-  A(S.unitPos, n + 1);
   A(S.chain, S.pairCapacity);
   A(S.unitOrder, n);
   A(S.counters, 16);

@@ -220,7 +220,39 @@ __global__ void __launch_bounds__(kBlock) k_partners_count(DevState S) {
 // Fill pass: small bodies copy their stash (or search again past kStash
 // partners) into their CSR list and sort it by the partners' before()
 // order; large bodies add their large-large partners.
-__global__ void __launch_bounds__(kBlock) k_partners_fill(DevState S) {
+// Sort key of a body for the units' before()-order sort: its minX order key
+// if it is a unit (the later box of >= 1 pair), all ones otherwise (after
+// every unit); the key's four digits go into the block's histogram.
+__device__ __forceinline__ void unit_key(uint32_t i, bool unit, float minX,
+                                         uint32_t *__restrict__ keys, uint32_t (*sh)[256],
+                                         uint32_t &units) {
+  const uint32_t k = unit ? float_order_key(minX) : 0xffffffffu;
+  keys[i] = k;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) atomicAdd(&sh[q][(k >> (8 * q)) & 255u], 1u);
+  units += unit ? 1u : 0u;
+}
+
+__device__ __forceinline__ void flush_unit_hist(uint32_t (*sh)[256], uint32_t units,
+                                                uint32_t *sUnits, uint32_t *hist,
+                                                uint32_t *unitCount) {
+  atomicAdd(sUnits, units);
+  __syncthreads();
+  for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
+    const uint32_t v = sh[i >> 8][i & 255];
+    if (v) atomicAdd(&hist[i], v);
+  }
+  if (threadIdx.x == 0 && *sUnits) atomicAdd(unitCount, *sUnits);
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_partners_fill(DevState S, uint32_t *__restrict__ keys, uint32_t *hist) {
+  __shared__ uint32_t sh[4][256];
+  __shared__ uint32_t sUnits;
+  for (int q = threadIdx.x; q < 4 * 256; q += blockDim.x) sh[q >> 8][q & 255] = 0;
+  if (threadIdx.x == 0) sUnits = 0;
+  __syncthreads();
+  uint32_t units = 0;
   const uint32_t n = S.n;
   const uint32_t mask = S.nBuckets - 1;
   const bool overflow = S.counters[0] > S.pairCapacity;
@@ -244,7 +276,7 @@ __global__ void __launch_bounds__(kBlock) k_partners_fill(DevState S) {
     }
     if (overflow) {
       S.nLater[i] = 0;
-      S.unitFlag[i] = 0;
+      unit_key(i, false, bi.x, keys, sh, units);
       if (i == 0) atomicOr(S.status, kStatusPairCapacity);
       continue;
     }
@@ -294,8 +326,9 @@ __global__ void __launch_bounds__(kBlock) k_partners_fill(DevState S) {
       if (before_key(S.box[u].x, u, bi.x, i)) ++nl;
     }
     S.nLater[i] = nl;
-    S.unitFlag[i] = nl > 0 ? 1u : 0u;
+    unit_key(i, nl > 0, bi.x, keys, sh, units);
   }
+  flush_unit_hist(sh, units, &sUnits, hist, &S.counters[1]);
 }
 
 // Small-large pairs recorded by the count pass, into the large lists.
@@ -312,7 +345,8 @@ __global__ void __launch_bounds__(kBlock) k_fill_large_pairs(DevState S) {
 
 // Sorts each large body's partner list (filled by others through atomics)
 // by before() order: one warp per large body, rank by counting.
-__global__ void __launch_bounds__(kBlock) k_sort_large(DevState S) {
+__global__ void __launch_bounds__(kBlock)
+    k_sort_large(DevState S, uint32_t *__restrict__ keys, uint32_t *hist) {
   const int lane = threadIdx.x & 31;
   const uint32_t warpId = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nWarps = (gridDim.x * blockDim.x) >> 5;
@@ -345,31 +379,21 @@ __global__ void __launch_bounds__(kBlock) k_sort_large(DevState S) {
         nl += before_key(S.box[u].x, u, gk, g) ? 1u : 0u;
       }
       for (int o = 16; o > 0; o >>= 1) nl += __shfl_xor_sync(0xffffffffu, nl, o);
-      if (lane == 0) {
-        S.nLater[g] = nl;
-        S.unitFlag[g] = nl > 0 ? 1u : 0u;
-      }
+      if (lane == 0) S.nLater[g] = nl;
     } else if (lane == 0) {
       S.nLater[g] = 0;
-      S.unitFlag[g] = 0;
+    }
+    if (lane == 0) {
+      // the large body's sort key (few bodies: straight to the histogram)
+      const bool unit = !overflow && d > 0 && S.nLater[g] > 0;
+      const uint32_t k = unit ? float_order_key(gk) : 0xffffffffu;
+      keys[g] = k;
+      for (int q = 0; q < 4; ++q) atomicAdd(&hist[q * 256 + ((k >> (8 * q)) & 255u)], 1u);
+      if (unit) atomicAdd(&S.counters[1], 1u);
     }
   }
 }
 
-// Units (bodies that are the later box of >= 1 pair), in index order, keyed
-// by their minX for the before()-order sort.
-__global__ void __launch_bounds__(kBlock) k_units(DevState S, uint32_t *keys,
-                                                  uint32_t *vals) {
-  const uint32_t n = S.n;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += gridDim.x * blockDim.x) {
-    if (S.unitFlag[i]) {
-      const uint32_t p = S.unitPos[i];
-      keys[p] = float_order_key(S.box[i].x);
-      vals[p] = i;
-    }
-  }
-}
 
 // resolve(bodies, i = later, j = earlier): Collision.cpp:16-84, IEEE op
 // for op.  s = {x, y, vx, vy}.
@@ -690,16 +714,17 @@ void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
   exclusive_scan_u32(s, S.deg, S.pstart, n, nullptr, &S.counters[0], scan,
                      S.status);
   mark(s, "collide.count");
-  k_partners_fill<<<grid_for(n), kBlock, 0, s>>>(S);
+  // the fill kernels also write every body's key for the units' sort
+  // (units first, in before() order) and its digit histograms
+  cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * 4 * 256, s);
+  cudaMemsetAsync(&S.counters[1], 0, sizeof(uint32_t), s);
+  k_partners_fill<<<grid_for(n), kBlock, 0, s>>>(S, keys32(sort, 0), sort.hist);
   k_fill_large_pairs<<<64, kBlock, 0, s>>>(S);
-  k_sort_large<<<64, kBlock, 0, s>>>(S);
+  k_sort_large<<<64, kBlock, 0, s>>>(S, keys32(sort, 0), sort.hist);
   mark(s, "collide.fill");
-  // units in before() order
-  exclusive_scan_u32(s, S.unitFlag, S.unitPos, n, nullptr, &S.counters[1],
-                     scan, S.status);
-  k_units<<<grid_for(n), kBlock, 0, s>>>(S, keys32(sort, 0), sort.vals[0]);
-  const int buf = radix_sort_u32(s, sort, n, &S.counters[1], 0, 32, false,
-                                 false, S.status);
+  // units in before() order: a stable sort of all bodies' keys (value =
+  // index), the first counters[1] entries being the units
+  const int buf = radix_sort_u32(s, sort, n, nullptr, 0, 32, true, true, S.status);
   mark(s, "collide.units");
   // ordered resolution
   cudaMemsetAsync(&S.counters[2], 0, sizeof(uint32_t), s);

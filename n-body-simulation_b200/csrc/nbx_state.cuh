@@ -99,8 +99,6 @@ struct DevState {
   uint2 *largePairs;     // (large, small) pairs found by the count pass
   uint32_t *fillLarge;   // fill counters of large bodies
   uint32_t *nLater;      // partners that sort before the body
-  uint32_t *unitFlag;    // nLater > 0
-  uint32_t *unitPos;     // scan of unitFlag
   uint32_t *unitOrder;   // units in before() order (last collide)
   uint32_t *longRuns;    // Morton sort: starts of runs of > 16 equal high keys
   uint32_t *counters;    // [0]=pairs*2 total [1]=units [2]=unit claim
