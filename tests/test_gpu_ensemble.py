@@ -87,10 +87,12 @@ def test_autotune_restores_state(nbx):
     # parameters bit for bit (grid and block shape change nothing; the leaf
     # width only the summation order, checked against the default below)
     h.step(3)
-    ref = nbx.Handle(sizes, theta=0.5, force_blocks=best["force_blocks"],
-                     force_block=best["force_block"], leaf_pairs=best["leaf_pairs"])
+    ref = nbx.Handle(sizes, theta=0.5)
     ref.upload(bodies)
-    ref.step(5)
+    ref.step(2)
+    ref.set_params(force_blocks=best["force_blocks"], force_block=best["force_block"],
+                   leaf_pairs=best["leaf_pairs"])
+    ref.step(3)
     assert same_bits(h.download(), ref.download())
     h.close()
     ref.close()
