@@ -388,7 +388,10 @@ int nbx_mlp_init(nbx_handle *h, uint32_t seed);
 /* Walks the last tree from the bodies at the given current indices with
  * MAC theta; every accepted cell with size/distance >= band yields a row
  * whose targets come from an FP64 direct sum over the cell's bodies.
- * Writes at most max_rows rows; *n_rows receives the number written. */
+ * Writes at most max_rows rows; *n_rows receives the number written.  The
+ * rows need the cells' second moments, which a tree built by nbx_phase
+ * (BUILD or ATTRACT) always has and a tree built by nbx_step only with
+ * use_mlp != 0 (otherwise NBX_ERR_STATE). */
 int nbx_mlp_harvest(nbx_handle *h, const uint32_t *targets, uint32_t n_targets,
                     float theta, float band, float *rows, uint32_t max_rows,
                     uint32_t *n_rows);

@@ -25,7 +25,7 @@ void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
                     SortScratch &sort);
 void launch_bounds(cudaStream_t s, const DevState &S);
 void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
-                  SortScratch &sort);
+                  SortScratch &sort, bool moments);
 void launch_bfs_tree(cudaStream_t s, const DevState &S, ScanScratch &scan,
                      SortScratch &sort);
 void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
@@ -245,6 +245,7 @@ struct nbx_handle {
   bool uploaded = false;
   bool treeValid = false;   // a Barnes-Hut tree of the current state exists
   bool bfsValid = false;    // its breadth-first arrays (built on demand)
+  bool momentsValid = false; // its cells' second moments were computed
   bool forceInput = false;  // S.xym holds the current state's bodies
   bool collideValid = false;
   bool idsChecked = false;     // ids verified to be per-instance permutations
@@ -502,7 +503,8 @@ DevState enqueue_step(nbx_handle *h, cudaStream_t s, DevState S) {
     mark(s, "forces");
     return S;
   }
-  launch_build(s, S, h->scan, h->sort);
+  // second moments only where the force pass reads them
+  launch_build(s, S, h->scan, h->sort, h->params.use_mlp != 0);
   if (h->timedCapture) cudaEventRecordWithFlags(h->forceMark[0], s, cudaEventRecordExternal);
   launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
                 h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
@@ -532,6 +534,7 @@ void destroy_graphs(nbx_handle *h) {
 void after_step(nbx_handle *h) {
   h->treeValid = h->params.force_law == 0;
   h->bfsValid = false;
+  h->momentsValid = h->params.use_mlp != 0; // what the step's build computed
   h->forceInput = true;
   h->collideValid = h->params.collisions != 0;
 }
@@ -1292,7 +1295,8 @@ int nbx_phase(nbx_handle *h, int phase) {
       h->forceInput = true;
       break;
     }
-    launch_build(s, S, h->scan, h->sort);
+    launch_build(s, S, h->scan, h->sort, true);
+    h->momentsValid = true;
     h->cur ^= 1;
     h->treeValid = true;
     h->bfsValid = false;
@@ -1319,7 +1323,8 @@ int nbx_phase(nbx_handle *h, int phase) {
       launch_naive_forces(s, S, h->params.exact_math != 0);
       break;
     }
-    launch_build(s, S, h->scan, h->sort);
+    launch_build(s, S, h->scan, h->sort, true);
+    h->momentsValid = true;
     h->cur ^= 1;
     h->treeValid = true;
     h->bfsValid = false;
@@ -1754,6 +1759,10 @@ int nbx_mlp_harvest(nbx_handle *h, const uint32_t *targets, uint32_t nt,
   if (!h || !nRows || (nt && !targets) || (maxRows && !rows)) return NBX_ERR_ARG;
   cudaSetDevice(h->device);
   if (!h->treeValid) return fail(h, NBX_ERR_STATE, "no tree built");
+  if (!h->momentsValid)
+    return fail(h, NBX_ERR_STATE,
+                "the last tree has no cell moments: build it with nbx_phase (BUILD or "
+                "ATTRACT), or step with use_mlp != 0");
   for (uint32_t k = 0; k < nt; ++k)
     if (targets[k] >= h->n) return fail(h, NBX_ERR_ARG, "target index out of range");
   *nRows = 0;

@@ -533,17 +533,6 @@ __global__ void __launch_bounds__(kBlock) k_trav_counts(DevState S) {
   }
 }
 
-// Record -> first body: body i owns records P_i .. P_i + count_i - 1.
-__global__ void __launch_bounds__(kBlock) k_trav_owner(DevState S, uint32_t *owner) {
-  const uint32_t total = S.counters[6];
-  if (total > S.nodeCapacity) return;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n;
-       i += gridDim.x * blockDim.x) {
-    const uint32_t cnt = S.splitCount[i], P = S.splitStart[i];
-    for (uint32_t k = 0; k < cnt; ++k) owner[P + k] = i;
-  }
-}
-
 // First index in (i, e] whose depth-d prefix differs from code[i]'s (pre),
 // given that the codes from e on all differ (a gallop, then a binary
 // search).  d >= 1.
@@ -681,6 +670,7 @@ __global__ void __launch_bounds__(kBlock)
 // (sumNode's order) and climbs; the last non-empty child to arrive sums its
 // parent's children in digit order, then finishNode's divide; second
 // moments about each centre of mass for the corrected forms.
+template <bool kMoments>
 __global__ void __launch_bounds__(kBlock)
     k_trav_upward(DevState S, const uint4 *__restrict__ kids) {
   const uint32_t total = S.counters[6];
@@ -699,18 +689,20 @@ __global__ void __launch_bounds__(kBlock)
     }
     const float div = fmaxf(mm, FLT_MIN);
     const float X = __fdiv_rn(px, div), Y = __fdiv_rn(py, div);
-    float ixx = 0.0f, iyy = 0.0f, ixy = 0.0f;
-    for (uint32_t b = b0; b < b1; ++b) {
-      const float4 q = S.xym[b];
-      const float dx = q.x - X, dy = q.y - Y;
-      ixx += q.z * dx * dx;
-      iyy += q.z * dy * dy;
-      ixy += q.z * dx * dy;
+    if (kMoments) {
+      float ixx = 0.0f, iyy = 0.0f, ixy = 0.0f;
+      for (uint32_t b = b0; b < b1; ++b) {
+        const float4 q = S.xym[b];
+        const float dx = q.x - X, dy = q.y - Y;
+        ixx += q.z * dx * dx;
+        iyy += q.z * dy * dy;
+        ixy += q.z * dx * dy;
+      }
+      __stcg(&S.tM[p], make_float4(ixx, iyy, ixy, S.tM[p].w));
     }
     __stcg(&S.sumX[p], px);
     __stcg(&S.sumY[p], py);
     __stcg(&S.tN[p].a, make_float4(X, Y, mm, S.tN[p].a.w));
-    __stcg(&S.tM[p], make_float4(ixx, iyy, ixy, S.tM[p].w));
     int32_t node = S.parent[p];
     for (int guard = 0; node >= 0 && guard <= kMaxDepth; ++guard) {
       const uint32_t g = (uint32_t)node;
@@ -736,7 +728,7 @@ __global__ void __launch_bounds__(kBlock)
         cxs[q] = __ldcg(&S.sumX[r[q]]);
         cys[q] = __ldcg(&S.sumY[r[q]]);
         ca[q] = __ldcg(&S.tN[r[q]].a);
-        mo[q] = __ldcg(&S.tM[r[q]]);
+        if (kMoments) mo[q] = __ldcg(&S.tM[r[q]]);
       }
       float sx = 0.0f, sy = 0.0f, sm = 0.0f;
       for (uint32_t q = 0; q < children && q < 4; ++q) {
@@ -747,18 +739,20 @@ __global__ void __launch_bounds__(kBlock)
       }
       const float dv = fmaxf(sm, FLT_MIN);
       const float PX = __fdiv_rn(sx, dv), PY = __fdiv_rn(sy, dv);
-      float jxx = 0.0f, jyy = 0.0f, jxy = 0.0f;
-      for (uint32_t q = 0; q < children && q < 4; ++q) {
-        if (r[q] >= total) break;
-        const float dx = ca[q].x - PX, dy = ca[q].y - PY;
-        jxx += mo[q].x + ca[q].z * dx * dx;
-        jyy += mo[q].y + ca[q].z * dy * dy;
-        jxy += mo[q].z + ca[q].z * dx * dy;
+      if (kMoments) {
+        float jxx = 0.0f, jyy = 0.0f, jxy = 0.0f;
+        for (uint32_t q = 0; q < children && q < 4; ++q) {
+          if (r[q] >= total) break;
+          const float dx = ca[q].x - PX, dy = ca[q].y - PY;
+          jxx += mo[q].x + ca[q].z * dx * dx;
+          jyy += mo[q].y + ca[q].z * dy * dy;
+          jxy += mo[q].z + ca[q].z * dx * dy;
+        }
+        __stcg(&S.tM[g], make_float4(jxx, jyy, jxy, S.tM[g].w));
       }
       __stcg(&S.sumX[g], sx);
       __stcg(&S.sumY[g], sy);
       __stcg(&S.tN[g].a, make_float4(PX, PY, sm, S.tN[g].a.w));
-      __stcg(&S.tM[g], make_float4(jxx, jyy, jxy, S.tM[g].w));
       node = S.parent[g];
     }
   }
@@ -767,10 +761,10 @@ __global__ void __launch_bounds__(kBlock)
 } // namespace
 
 void launch_bounds(cudaStream_t s, const DevState &S);
-void launch_trav_tree(cudaStream_t s, const DevState &S, ScanScratch &scan);
+void launch_trav_tree(cudaStream_t s, const DevState &S, ScanScratch &scan, bool moments);
 
 void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
-                  SortScratch &sort) {
+                  SortScratch &sort, bool moments) {
   const uint32_t n = S.n;
   launch_bounds(s, S);
   k_root_frame<<<(S.nseg + 127) / 128, 128, 0, s>>>(S);
@@ -809,23 +803,28 @@ void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
   T.mr2 = S.mr;
   T.id2 = S.id;
   S = T;
-  launch_trav_tree(s, S, scan);
+  launch_trav_tree(s, S, scan, moments);
 }
 
 // The traversal layout straight from the sorted codes (the step path).
-void launch_trav_tree(cudaStream_t s, const DevState &S, ScanScratch &scan) {
+// moments: the cells' second moments too (only the corrected forms and the
+// network's harvest read them).
+void launch_trav_tree(cudaStream_t s, const DevState &S, ScanScratch &scan, bool moments) {
   const uint32_t n = S.n;
-  k_trav_counts<<<grid_for(n), kBlock, 0, s>>>(S);
-  exclusive_scan_u32(s, S.splitCount, S.splitStart, n, nullptr, &S.counters[6],
-                     scan, S.status);
-  mark(s, "tree.counts");
   // per-record scratch in arrays only the breadth-first build uses
   uint32_t *owner = reinterpret_cast<uint32_t *>(S.start);
   uint4 *kids = reinterpret_cast<uint4 *>(S.moments);
-  k_trav_owner<<<grid_for(n), kBlock, 0, s>>>(S, owner);
+  k_trav_counts<<<grid_for(n), kBlock, 0, s>>>(S);
+  // the scan also writes each record's first body (owner)
+  exclusive_scan_u32(s, S.splitCount, S.splitStart, n, nullptr, &S.counters[6],
+                     scan, S.status, owner, S.nodeCapacity);
+  mark(s, "tree.counts");
   k_trav_nodes<<<grid_for(n / 2 + 64), kBlock, 0, s>>>(S, owner, kids);
   mark(s, "tree.nodes");
-  k_trav_upward<<<grid_for(n / 4 + 64), kBlock, 0, s>>>(S, kids);
+  if (moments)
+    k_trav_upward<true><<<grid_for(n / 4 + 64), kBlock, 0, s>>>(S, kids);
+  else
+    k_trav_upward<false><<<grid_for(n / 4 + 64), kBlock, 0, s>>>(S, kids);
   mark(s, "tree.upward");
 }
 

@@ -105,10 +105,13 @@ constexpr int kScanItems = 16;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
 // out[i] = sum(in[0..i)) for i < n; if total != nullptr it receives the sum.
-// n is *d_n when d_n != nullptr (n_max bounds the launch).
+// n is *d_n when d_n != nullptr (n_max bounds the launch).  With owner,
+// owner[out[i] + k] = i for k < in[i] (below owner_cap): the element that
+// each unit of the scanned counts belongs to.
 void exclusive_scan_u32(cudaStream_t s, const uint32_t *in, uint32_t *out,
                         uint32_t n_max, const uint32_t *d_n, uint32_t *total,
-                        ScanScratch &sc, uint32_t *err);
+                        ScanScratch &sc, uint32_t *err, uint32_t *owner = nullptr,
+                        uint32_t owner_cap = 0);
 size_t scan_scratch_tiles(uint32_t n_max);
 
 constexpr int kSortThreads = 256;

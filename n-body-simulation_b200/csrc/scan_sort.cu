@@ -58,7 +58,8 @@ __global__ void __launch_bounds__(kScanThreads)
 __global__ void __launch_bounds__(kScanThreads)
     k_scan_apply(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
                  uint32_t n_max, const uint32_t *d_n, uint32_t *total,
-                 const uint32_t *__restrict__ tileSum) {
+                 const uint32_t *__restrict__ tileSum, uint32_t *__restrict__ owner,
+                 uint32_t ownerCap) {
   __shared__ uint32_t s_items[kScanTile];
   __shared__ uint32_t s_warp[kScanThreads / 32];
   __shared__ uint32_t sh[kScanThreads / 32];
@@ -112,7 +113,14 @@ __global__ void __launch_bounds__(kScanThreads)
   __syncthreads();
   for (int k = 0; k < kScanItems; ++k) {
     const uint32_t i = base + k * kScanThreads + tid;
-    if (i < n) out[i] = s_items[k * kScanThreads + tid];
+    if (i < n) {
+      const uint32_t o = s_items[k * kScanThreads + tid];
+      out[i] = o;
+      if (owner) {
+        const uint32_t c = in[i];
+        for (uint32_t j = 0; j < c && o + j < ownerCap; ++j) owner[o + j] = i;
+      }
+    }
   }
 }
 
@@ -124,7 +132,8 @@ size_t scan_scratch_tiles(uint32_t n_max) {
 
 void exclusive_scan_u32(cudaStream_t s, const uint32_t *in, uint32_t *out,
                         uint32_t n_max, const uint32_t *d_n, uint32_t *total,
-                        ScanScratch &sc, uint32_t *err) {
+                        ScanScratch &sc, uint32_t *err, uint32_t *owner,
+                        uint32_t owner_cap) {
   const uint32_t tiles = (n_max + kScanTile - 1) / kScanTile;
   uint32_t *tileSum = reinterpret_cast<uint32_t *>(sc.status);
   (void)err;
@@ -132,7 +141,7 @@ void exclusive_scan_u32(cudaStream_t s, const uint32_t *in, uint32_t *out,
   if (tiles > 1)
     k_scan_reduce<<<tiles, kScanThreads, 0, s>>>(in, n_max, d_n, tileSum);
   k_scan_apply<<<tiles > 0 ? tiles : 1, kScanThreads, 0, s>>>(in, out, n_max, d_n, total,
-                                                               tileSum);
+                                                               tileSum, owner, owner_cap);
 }
 
 // ------------------------------------------------------------ radix sort
@@ -179,8 +188,10 @@ __global__ void k_radix_hist_scan(uint32_t *hist, int pass_lo) {
   h[t] = s[t] - h[t];
 }
 
+// At least 3 blocks per SM (<= 85 registers): a 1M-key pass (342 tiles)
+// is then resident in one wave on 148 SMs.
 template <typename K, bool kIdentity>
-__global__ void __launch_bounds__(kSortThreads)
+__global__ void __launch_bounds__(kSortThreads, 3)
     k_onesweep(const K *__restrict__ keysIn,
                const uint32_t *__restrict__ valsIn,
                K *__restrict__ keysOut, uint32_t *__restrict__ valsOut,
