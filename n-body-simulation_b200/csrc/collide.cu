@@ -59,6 +59,36 @@ __device__ __forceinline__ uint32_t cell_hash(uint32_t seg, int cx, int cy,
   return ((x | (y << 1)) + hi + seg * 0x2545F491u) & mask;
 }
 
+// cell_hash of the 3x3 cells around (cx, cy), row by row from (cx-1, cy-1):
+// the coordinates are interleaved once and their neighbours stepped in
+// interleaved form (add or subtract 1 across the gaps of the spread bits),
+// so h[k] == cell_hash(seg, cx + k % 3 - 1, cy + k / 3 - 1, mask).
+__device__ __forceinline__ uint32_t spread16(uint32_t x) {
+  x &= 0xffffu;
+  x = (x | (x << 8)) & 0x00FF00FFu;
+  x = (x | (x << 4)) & 0x0F0F0F0Fu;
+  x = (x | (x << 2)) & 0x33333333u;
+  return (x | (x << 1)) & 0x55555555u;
+}
+__device__ __forceinline__ void cell_hash3x3(uint32_t seg, int cx, int cy, uint32_t mask,
+                                             uint32_t h[9]) {
+  const uint32_t dx = spread16((uint32_t)cx), dy = spread16((uint32_t)cy);
+  const uint32_t xs[3] = {((dx & 0x55555555u) - 1u) & 0x55555555u, dx,
+                          ((dx | 0xAAAAAAAAu) + 1u) & 0x55555555u};
+  const uint32_t ys[3] = {((dy & 0x55555555u) - 1u) & 0x55555555u, dy,
+                          ((dy | 0xAAAAAAAAu) + 1u) & 0x55555555u};
+  const uint32_t so = seg * 0x2545F491u;
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    const uint32_t hy = ((uint32_t)(cy + b - 1) >> 16) * 0x85EBCA77u;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const uint32_t hx = ((uint32_t)(cx + a - 1) >> 16) * 0x9E3779B1u;
+      h[3 * b + a] = ((xs[a] | (ys[b] << 1)) + (hx ^ hy) + so) & mask;
+    }
+  }
+}
+
 // floor of the exact product v*inv (the reference takes the floor of the
 // double product, Collision.cpp:100-104).
 __device__ __forceinline__ int exact_floor_mul(float v, float inv) {
@@ -177,10 +207,12 @@ __global__ void __launch_bounds__(kBlock) k_partners_count(DevState S) {
     uint32_t *stash = S.stash + (size_t)i * kStash;
     if (!(S.slot[i] & 0x80000000u)) {
       const int2 c = S.cellXY[i];
+      uint32_t hs[9];
+      cell_hash3x3(sg, c.x, c.y, mask, hs);
       for (int dy = -1; dy <= 1; ++dy) {
         for (int dx = -1; dx <= 1; ++dx) {
           const int ncx = c.x + dx, ncy = c.y + dy;
-          const uint32_t h = cell_hash(sg, ncx, ncy, mask);
+          const uint32_t h = hs[3 * (dy + 1) + (dx + 1)];
           const uint32_t e0 = S.bucketStart[h], e1 = S.bucketStart[h + 1];
           for (uint32_t e = e0; e < e1; ++e) {
             const uint32_t j = S.grid[e];
@@ -288,10 +320,12 @@ __global__ void __launch_bounds__(kBlock)
     } else {
       uint32_t w = 0;
       const int2 c = S.cellXY[i];
+      uint32_t hs[9];
+      cell_hash3x3(sg, c.x, c.y, mask, hs);
       for (int dy = -1; dy <= 1; ++dy) {
         for (int dx = -1; dx <= 1; ++dx) {
           const int ncx = c.x + dx, ncy = c.y + dy;
-          const uint32_t h = cell_hash(sg, ncx, ncy, mask);
+          const uint32_t h = hs[3 * (dy + 1) + (dx + 1)];
           const uint32_t e0 = S.bucketStart[h], e1 = S.bucketStart[h + 1];
           for (uint32_t e = e0; e < e1; ++e) {
             const uint32_t j = S.grid[e];
