@@ -75,6 +75,16 @@ __global__ void k_root_frame(DevState S) {
   b[3] = 0u;
 }
 
+// quantise() in native FP64 (TreeKernels.cuh:48-57): one IEEE subtract and
+// one multiply, each rounded (no contraction), then floor -- the same
+// doubles as the reference's, bit for bit, from the frame's binary64 bits.
+__device__ __forceinline__ uint32_t quantise_fp64(float v, double lo, double scale) {
+  const double q = floor(__dmul_rn(__dsub_rn((double)v, lo), scale));
+  if (!(q > 0.0)) return 0u; // also NaN
+  if (q >= 4294967295.0) return 0xFFFFFFFFu;
+  return (uint32_t)q;
+}
+
 // Morton code of every body; the sort key is its high half (depth-16
 // cells), with the digit histograms of its four radix passes fused.
 __global__ void __launch_bounds__(kBlock)
@@ -87,7 +97,10 @@ __global__ void __launch_bounds__(kBlock)
        i += gridDim.x * blockDim.x) {
     const float4 p = S.pv[i];
     const MortonFrame f = S.seg[S.segOf[i]].frame;
-    const uint64_t c = morton_code(p.x, p.y, f);
+    const double sc = __longlong_as_double((long long)f.scale);
+    const uint64_t c =
+        (spread_bits(quantise_fp64(p.y, __longlong_as_double((long long)f.y0), sc)) << 1) |
+        spread_bits(quantise_fp64(p.x, __longlong_as_double((long long)f.x0), sc));
     const uint32_t k = (uint32_t)(c >> 32);
     keys[i] = k;
     S.codes[i] = c;

@@ -7,10 +7,11 @@
 //  * sd_*: IEEE-754 binary64 add/sub/mul/div and floor done with 64-bit
 //    integer arithmetic (round to nearest, ties to even).  The reference
 //    quantises Morton coordinates in double
-//    (src/cuda/TreeKernels.cuh:48-57, CudaQuadTree.cu:41-44); the kernels
-//    reproduce those doubles bit for bit without using the FP64 units,
-//    which this design keeps for the FP64 direct-sum check and the drift
-//    reductions only.
+//    (src/cuda/TreeKernels.cuh:48-57, CudaQuadTree.cu:41-44); these
+//    reproduce those doubles bit for bit anywhere, host included: the
+//    per-instance Morton frame is made with them, and the host checks use
+//    them.  The per-body quantisation of the step runs in native FP64
+//    (build.cu), which rounds the same IEEE operations the same way.
 //  * fast_inv_sqrt: the force law's bit-level inverse square root
 //    (src/QuadTree.cpp:11-26, TreeKernels.cuh:180-195).
 //  * float_order_key: a float's total-order key for radix sorting.
