@@ -604,7 +604,9 @@ __device__ __forceinline__ uint32_t record_of(const DevState &S, uint32_t b, int
 // One thread per record: body range, next and open slots, size and centre
 // (splitNode's arithmetic along the path), parent, the records of the
 // non-empty children in digit order (all ones past the last); arrival
-// counters cleared.
+// counters cleared.  kFull: also the cell centres and sizes of tC/tM (read
+// only by the corrected forms and the network's harvest).
+template <bool kFull>
 __global__ void __launch_bounds__(kBlock)
     k_trav_nodes(DevState S, const uint32_t *__restrict__ owner, uint4 *__restrict__ kids) {
   const uint64_t *c = S.sortedCodes;
@@ -635,11 +637,17 @@ __global__ void __launch_bounds__(kBlock)
     const bool leaf = k + 1 == S.splitCount[i];
     const uint64_t ci = c[i];
     float cx = G.cx, cy = G.cy, size = G.size;
-    for (int t = 0; t < d; ++t) {
-      size = __fmul_rn(size, 0.5f);
-      const int q = digit_at(ci, t);
-      cx = __fadd_rn(cx, __fmul_rn((float)(q & 1) - 0.5f, size));
-      cy = __fadd_rn(cy, __fmul_rn((float)(q >> 1) - 0.5f, size));
+    if (kFull || !(fabsf(G.size) >= 0x1p-90f && fabsf(G.size) <= 0x1p+120f)) {
+      for (int t = 0; t < d; ++t) {
+        size = __fmul_rn(size, 0.5f);
+        const int q = digit_at(ci, t);
+        cx = __fadd_rn(cx, __fmul_rn((float)(q & 1) - 0.5f, size));
+        cy = __fadd_rn(cy, __fmul_rn((float)(q >> 1) - 0.5f, size));
+      }
+    } else {
+      // d <= 32 halvings of a normal size stay normal: each is exact, so
+      // the repeated halving is one exponent step
+      size = ldexpf(size, -d);
     }
     const uint32_t e = d > 0 ? prefix_end(c, i, s1, d, ci >> (64 - 2 * d)) : s1;
     // the record after the subtree; all ones past the instance's last
@@ -670,8 +678,10 @@ __global__ void __launch_bounds__(kBlock)
     TravNode &T = S.tN[p];
     T.a = make_float4(0.0f, 0.0f, 0.0f, __fmul_rn(size, size));
     T.b = make_int4((int)next, (int)(leaf ? next : p + 1), (int)i, (int)e);
-    S.tM[p] = make_float4(0.0f, 0.0f, 0.0f, size);
-    S.tC[p] = make_float2(cx, cy);
+    if (kFull) {
+      S.tM[p] = make_float4(0.0f, 0.0f, 0.0f, size);
+      S.tC[p] = make_float2(cx, cy);
+    }
     S.parent[p] = parent;
     S.subtree[p] = children;
     S.arrive[p] = 0u;
@@ -820,8 +830,8 @@ void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
 }
 
 // The traversal layout straight from the sorted codes (the step path).
-// moments: the cells' second moments too (only the corrected forms and the
-// network's harvest read them).
+// moments: the cells' second moments, centres and sizes too (tM, tC: only
+// the corrected forms and the network's harvest read them).
 void launch_trav_tree(cudaStream_t s, const DevState &S, ScanScratch &scan, bool moments) {
   const uint32_t n = S.n;
   // per-record scratch in arrays only the breadth-first build uses
@@ -832,7 +842,10 @@ void launch_trav_tree(cudaStream_t s, const DevState &S, ScanScratch &scan, bool
   exclusive_scan_u32(s, S.splitCount, S.splitStart, n, nullptr, &S.counters[6],
                      scan, S.status, owner, S.nodeCapacity);
   mark(s, "tree.counts");
-  k_trav_nodes<<<grid_for(n / 2 + 64), kBlock, 0, s>>>(S, owner, kids);
+  if (moments)
+    k_trav_nodes<true><<<grid_for(n / 2 + 64), kBlock, 0, s>>>(S, owner, kids);
+  else
+    k_trav_nodes<false><<<grid_for(n / 2 + 64), kBlock, 0, s>>>(S, owner, kids);
   mark(s, "tree.nodes");
   if (moments)
     k_trav_upward<true><<<grid_for(n / 4 + 64), kBlock, 0, s>>>(S, kids);

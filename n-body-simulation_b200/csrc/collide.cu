@@ -768,7 +768,7 @@ void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
 }
 
 void launch_bounds(cudaStream_t s, const DevState &S) {
-  uint32_t blocks = (S.n + 4095) / 4096;
+  uint32_t blocks = (S.n + 1023) / 1024; // 4 bodies per thread
   if (blocks > 148u * 8u) blocks = 148u * 8u;
   if (blocks < 1) blocks = 1;
   k_bounds<<<blocks, kBlock, 0, s>>>(S);
