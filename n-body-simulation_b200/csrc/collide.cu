@@ -252,16 +252,32 @@ __global__ void __launch_bounds__(kBlock) k_partners_count(DevState S) {
 // Fill pass: small bodies copy their stash (or search again past kStash
 // partners) into their CSR list and sort it by the partners' before()
 // order; large bodies add their large-large partners.
-// Sort key of a body for the units' before()-order sort: its minX order key
-// if it is a unit (the later box of >= 1 pair), all ones otherwise (after
-// every unit); the key's four digits go into the block's histogram.
-__device__ __forceinline__ void unit_key(uint32_t i, bool unit, float minX,
+// Coarse sort key of a unit's minX: 24 bits over twice the instance's last
+// root square, order-preserving (a float subtract, a multiply by a positive
+// scale and floor are each monotone), clamped at the ends.  The sort on it
+// is completed by ordering each run of equal keys by the exact minX
+// (sort_fix_units), so only speed depends on how well it spreads.
+constexpr uint32_t kUnitKeyMax = (1u << 24) - 2;  // largest unit key
+constexpr uint32_t kNonUnitKey = (1u << 24) - 1;  // every non-unit, last
+__device__ __forceinline__ uint32_t unit_coarse_key(const SegDev &G, float minX) {
+  const float lo = G.cx - G.size;
+  const float scale = G.size > 0.0f && G.size <= 1e30f ? (float)kUnitKeyMax / (2.0f * G.size)
+                                                       : 0.0f;
+  const float q = floorf((minX - lo) * scale);
+  if (!(q > 0.0f)) return 0u;
+  return q >= (float)kUnitKeyMax ? kUnitKeyMax : (uint32_t)q;
+}
+
+// Sort key of a body for the units' before()-order sort: its coarse minX
+// key if it is a unit (the later box of >= 1 pair), kNonUnitKey otherwise
+// (after every unit); the key's three digits go into the block's histogram.
+__device__ __forceinline__ void unit_key(uint32_t i, bool unit, const SegDev &G, float minX,
                                          uint32_t *__restrict__ keys, uint32_t (*sh)[256],
                                          uint32_t &units) {
-  const uint32_t k = unit ? float_order_key(minX) : 0xffffffffu;
+  const uint32_t k = unit ? unit_coarse_key(G, minX) : kNonUnitKey;
   keys[i] = k;
 #pragma unroll
-  for (int q = 0; q < 4; ++q) atomicAdd(&sh[q][(k >> (8 * q)) & 255u], 1u);
+  for (int q = 0; q < 3; ++q) atomicAdd(&sh[q][(k >> (8 * q)) & 255u], 1u);
   units += unit ? 1u : 0u;
 }
 
@@ -270,7 +286,7 @@ __device__ __forceinline__ void flush_unit_hist(uint32_t (*sh)[256], uint32_t un
                                                 uint32_t *unitCount) {
   atomicAdd(sUnits, units);
   __syncthreads();
-  for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
+  for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) {
     const uint32_t v = sh[i >> 8][i & 255];
     if (v) atomicAdd(&hist[i], v);
   }
@@ -279,9 +295,9 @@ __device__ __forceinline__ void flush_unit_hist(uint32_t (*sh)[256], uint32_t un
 
 __global__ void __launch_bounds__(kBlock)
     k_partners_fill(DevState S, uint32_t *__restrict__ keys, uint32_t *hist) {
-  __shared__ uint32_t sh[4][256];
+  __shared__ uint32_t sh[3][256];
   __shared__ uint32_t sUnits;
-  for (int q = threadIdx.x; q < 4 * 256; q += blockDim.x) sh[q >> 8][q & 255] = 0;
+  for (int q = threadIdx.x; q < 3 * 256; q += blockDim.x) sh[q >> 8][q & 255] = 0;
   if (threadIdx.x == 0) sUnits = 0;
   __syncthreads();
   uint32_t units = 0;
@@ -308,7 +324,7 @@ __global__ void __launch_bounds__(kBlock)
     }
     if (overflow) {
       S.nLater[i] = 0;
-      unit_key(i, false, bi.x, keys, sh, units);
+      unit_key(i, false, S.seg[sg], bi.x, keys, sh, units);
       if (i == 0) atomicOr(S.status, kStatusPairCapacity);
       continue;
     }
@@ -360,7 +376,7 @@ __global__ void __launch_bounds__(kBlock)
       if (before_key(S.box[u].x, u, bi.x, i)) ++nl;
     }
     S.nLater[i] = nl;
-    unit_key(i, nl > 0, bi.x, keys, sh, units);
+    unit_key(i, nl > 0, S.seg[sg], bi.x, keys, sh, units);
   }
   flush_unit_hist(sh, units, &sUnits, hist, &S.counters[1]);
 }
@@ -420,9 +436,9 @@ __global__ void __launch_bounds__(kBlock)
     if (lane == 0) {
       // the large body's sort key (few bodies: straight to the histogram)
       const bool unit = !overflow && d > 0 && S.nLater[g] > 0;
-      const uint32_t k = unit ? float_order_key(gk) : 0xffffffffu;
+      const uint32_t k = unit ? unit_coarse_key(S.seg[S.segOf[g]], gk) : kNonUnitKey;
       keys[g] = k;
-      for (int q = 0; q < 4; ++q) atomicAdd(&hist[q * 256 + ((k >> (8 * q)) & 255u)], 1u);
+      for (int q = 0; q < 3; ++q) atomicAdd(&hist[q * 256 + ((k >> (8 * q)) & 255u)], 1u);
       if (unit) atomicAdd(&S.counters[1], 1u);
     }
   }
@@ -750,15 +766,18 @@ void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
   mark(s, "collide.count");
   // the fill kernels also write every body's key for the units' sort
   // (units first, in before() order) and its digit histograms
-  cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * 4 * 256, s);
+  cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * 3 * 256, s);
   cudaMemsetAsync(&S.counters[1], 0, sizeof(uint32_t), s);
   k_partners_fill<<<grid_for(n), kBlock, 0, s>>>(S, keys32(sort, 0), sort.hist);
   k_fill_large_pairs<<<64, kBlock, 0, s>>>(S);
   k_sort_large<<<64, kBlock, 0, s>>>(S, keys32(sort, 0), sort.hist);
   mark(s, "collide.fill");
-  // units in before() order: a stable sort of all bodies' keys (value =
-  // index), the first counters[1] entries being the units
-  const int buf = radix_sort_u32(s, sort, n, nullptr, 0, 32, true, true, S.status);
+  // units in before() order: a stable sort of all bodies' coarse keys
+  // (value = index), then each run of equal coarse keys in exact minX order;
+  // the first counters[1] entries are the units
+  const int buf = radix_sort_u32(s, sort, n, nullptr, 0, 24, true, true, S.status);
+  sort_fix_units(s, sort, buf, n, S.box, kNonUnitKey, S.longRuns, &S.counters[9],
+                 n / 16 + 64, S.status);
   mark(s, "collide.units");
   // ordered resolution
   cudaMemsetAsync(&S.counters[2], 0, sizeof(uint32_t), s);

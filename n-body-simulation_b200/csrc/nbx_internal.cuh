@@ -158,4 +158,12 @@ void sort_fix_low_bits32(cudaStream_t s, SortScratch &sc, int buf, uint32_t n,
                          const uint64_t *codes, uint32_t *longRuns, uint32_t *runCount,
                          uint32_t cap, uint32_t *err);
 
+// The same for the contact units, whose radix passes ran on a coarse,
+// order-preserving key of the box's minX: every run of equal coarse keys
+// (but the `skip` run of non-units) is put in order of the exact minX
+// order key, stably (ties keep index order).
+void sort_fix_units(cudaStream_t s, SortScratch &sc, int buf, uint32_t n, const float4 *box,
+                    uint32_t skip, uint32_t *longRuns, uint32_t *runCount, uint32_t cap,
+                    uint32_t *err);
+
 } // namespace nbx

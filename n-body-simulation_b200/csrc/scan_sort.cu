@@ -354,18 +354,33 @@ __global__ void __launch_bounds__(kSortThreads, 3)
 
 constexpr uint32_t kShortRun = 16; // runs up to this length: one thread
 
-// 32-bit keys (the high halves of 64-bit codes): every run of equal keys is
-// put in order of the codes' low halves, stably, in place in vals.  Runs of
-// up to kShortRun are insertion-sorted by the thread at their start; longer
-// ones are listed for k_long_runs32.
+// The key that orders the elements of a run of equal sort keys, from the
+// element's value: the low half of its Morton code, or the order key of its
+// box's minX.
+struct CodeLow {
+  const uint64_t *codes;
+  __device__ uint32_t operator()(uint32_t v) const { return (uint32_t)codes[v]; }
+};
+struct BoxMinX {
+  const float4 *box;
+  __device__ uint32_t operator()(uint32_t v) const { return float_order_key(box[v].x); }
+};
+
+// Every run of equal keys is put in order of the elements' in-run keys
+// (lk), stably, in place in vals; with hasSkip, a run of `skip` keys is
+// left as it is.
+// Runs of up to kShortRun are insertion-sorted by the thread at their
+// start; longer ones are listed for k_long_runs32.
+template <class LowKey>
 __global__ void __launch_bounds__(256)
     k_fix_runs32(const uint32_t *__restrict__ keys, uint32_t *__restrict__ vals,
-                 uint32_t n, const uint64_t *__restrict__ codes,
+                 uint32_t n, LowKey lowKey, bool hasSkip, uint32_t skip,
                  uint32_t *__restrict__ longRuns, uint32_t *longCount, uint32_t cap,
                  uint32_t *err) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += gridDim.x * blockDim.x) {
     const uint32_t hi = keys[i];
+    if (hasSkip && hi == skip) continue;
     if (i > 0 && keys[i - 1] == hi) continue;      // not a run start
     if (i + 1 >= n || keys[i + 1] != hi) continue; // single key
     uint32_t len = 2;
@@ -379,7 +394,7 @@ __global__ void __launch_bounds__(256)
     uint32_t lk[kShortRun], v[kShortRun];
     for (uint32_t a = 0; a < len; ++a) {
       v[a] = vals[i + a];
-      lk[a] = (uint32_t)codes[v[a]];
+      lk[a] = lowKey(v[a]);
     }
     for (uint32_t a = 1; a < len; ++a) { // stable: equal keys keep their order
       const uint32_t kk = lk[a], vv = v[a];
@@ -396,13 +411,14 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// One block per long run: its keys are replaced by the codes' low halves, a
+// One block per long run: its keys are replaced by the in-run keys, a
 // stable LSD radix sort (4 passes, through the other buffer over the same
 // index range) orders the run, and the keys are restored.
+template <class LowKey>
 __global__ void __launch_bounds__(256)
     k_long_runs32(uint32_t *__restrict__ keys, uint32_t *__restrict__ vals,
                   uint32_t *__restrict__ tmpK, uint32_t *__restrict__ tmpV, uint32_t n,
-                  const uint64_t *__restrict__ codes, const uint32_t *__restrict__ longRuns,
+                  LowKey lowKey, const uint32_t *__restrict__ longRuns,
                   const uint32_t *longCount, uint32_t cap) {
   __shared__ uint32_t sHist[256], sOff[256], sWarp[8][256];
   __shared__ uint32_t sEnd;
@@ -423,7 +439,7 @@ __global__ void __launch_bounds__(256)
       if (found) break;
     }
     const uint32_t e0 = sEnd;
-    for (uint32_t i = s0 + tid; i < e0; i += 256) keys[i] = (uint32_t)codes[vals[i]];
+    for (uint32_t i = s0 + tid; i < e0; i += 256) keys[i] = lowKey(vals[i]);
     __syncthreads();
     uint32_t *srcK = keys, *dstK = tmpK, *srcV = vals, *dstV = tmpV;
     for (int p = 0; p < 4; ++p) {
@@ -497,10 +513,25 @@ void sort_fix_low_bits32(cudaStream_t s, SortScratch &sc, int buf, uint32_t n,
   cudaMemsetAsync(runCount, 0, sizeof(uint32_t), s);
   uint32_t b = (n + 255) / 256;
   if (b > 148u * 16u) b = 148u * 16u;
-  k_fix_runs32<<<b, 256, 0, s>>>(keys32(sc, buf), sc.vals[buf], n, codes, longRuns, runCount,
-                                 cap, err);
+  const CodeLow lk{codes};
+  k_fix_runs32<<<b, 256, 0, s>>>(keys32(sc, buf), sc.vals[buf], n, lk, false, 0u, longRuns,
+                                 runCount, cap, err);
   k_long_runs32<<<148, 256, 0, s>>>(keys32(sc, buf), sc.vals[buf], keys32(sc, buf ^ 1),
-                                     sc.vals[buf ^ 1], n, codes, longRuns, runCount, cap);
+                                     sc.vals[buf ^ 1], n, lk, longRuns, runCount, cap);
+}
+
+void sort_fix_units(cudaStream_t s, SortScratch &sc, int buf, uint32_t n, const float4 *box,
+                    uint32_t skip, uint32_t *longRuns, uint32_t *runCount, uint32_t cap,
+                    uint32_t *err) {
+  if (n < 2) return;
+  cudaMemsetAsync(runCount, 0, sizeof(uint32_t), s);
+  uint32_t b = (n + 255) / 256;
+  if (b > 148u * 16u) b = 148u * 16u;
+  const BoxMinX lk{box};
+  k_fix_runs32<<<b, 256, 0, s>>>(keys32(sc, buf), sc.vals[buf], n, lk, true, skip, longRuns,
+                                 runCount, cap, err);
+  k_long_runs32<<<148, 256, 0, s>>>(keys32(sc, buf), sc.vals[buf], keys32(sc, buf ^ 1),
+                                     sc.vals[buf ^ 1], n, lk, longRuns, runCount, cap);
 }
 
 size_t sort_tiles(uint32_t n_max) {
