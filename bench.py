@@ -74,6 +74,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true",
                     help="headline workload only (no learned/ensemble legs)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="default launch parameters (profiling: no tuner trials "
+                         "before the timed steps)")
     return ap.parse_args()
 
 
@@ -589,7 +592,8 @@ def run_b200(args):
     # the library's autotuner picks the force walk's block shape, leaf width
     # and grid for this workload (leaf capacity stays the reference's 16);
     # it restores the state it timed from
-    tuned = sim.autotune(allow_leaf=False, steps=3)
+    tuned = (sim.autotune(allow_leaf=False, steps=3) if not args.no_autotune else
+             {"force_block": 0, "leaf_pairs": 1, "force_blocks": 0, "leaf_capacity": 16})
     sim.step(args.warmup)
     sim.sync()
     kernels_per_step = sim.step_kernels()
