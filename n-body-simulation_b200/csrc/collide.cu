@@ -183,12 +183,47 @@ __global__ void __launch_bounds__(kBlock) k_fill_grid(DevState S) {
     } else {
       const int2 c = S.cellXY[i];
       const uint32_t h = cell_hash(sg, c.x, c.y, S.nBuckets - 1);
-      S.grid[S.bucketStart[h] + s] = i;
+      const uint32_t e = S.bucketStart[h] + s;
+      S.grid[e] = i;
+      S.gridBox[e] = S.box[i];
     }
   }
 }
 
 constexpr uint32_t kStash = 16; // partners remembered per body by the count pass
+
+// Every small body of the same instance whose box overlaps small body i's,
+// from the buckets of the 3x3 cells around i's cell: f(j) for each, in
+// bucket order.  A bucket shared by two of the nine cells is read once.
+// Bodies of other cells that share a bucket need no cell test: two small
+// boxes that overlap lie in cells at most one apart on each axis (a box is
+// at most 0.999 of a cell wide and the cell index is the exact floor), so a
+// body from any other cell fails the overlap test by itself.  The boxes are
+// read beside the indices (gridBox), so a candidate costs no dependent load.
+template <class F>
+__device__ __forceinline__ void for_each_cell_neighbour(const DevState &S, uint32_t i,
+                                                        uint32_t sg, const float4 &bi,
+                                                        uint32_t mask, F &&f) {
+  const int2 c = S.cellXY[i];
+  uint32_t hs[9];
+  cell_hash3x3(sg, c.x, c.y, mask, hs);
+  const bool oneInstance = S.nseg == 1;
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    bool seen = false;
+#pragma unroll
+    for (int r = 0; r < q; ++r) seen |= hs[r] == hs[q];
+    if (seen) continue;
+    const uint32_t e0 = S.bucketStart[hs[q]], e1 = S.bucketStart[hs[q] + 1];
+    for (uint32_t e = e0; e < e1; ++e) {
+      const uint32_t j = S.grid[e];
+      const float4 bj = S.gridBox[e];
+      if (j == i) continue;
+      if (!oneInstance && S.segOf[j] != sg) continue;
+      if (boxes_overlap(bi, i, bj, j)) f(j);
+    }
+  }
+}
 
 // Partner discovery, count pass: every overlap of a small body's box in its
 // 3x3 cell neighbourhood and with the large boxes of its instance.  The
@@ -206,26 +241,10 @@ __global__ void __launch_bounds__(kBlock) k_partners_count(DevState S) {
     uint32_t cnt = 0;
     uint32_t *stash = S.stash + (size_t)i * kStash;
     if (!(S.slot[i] & 0x80000000u)) {
-      const int2 c = S.cellXY[i];
-      uint32_t hs[9];
-      cell_hash3x3(sg, c.x, c.y, mask, hs);
-      for (int dy = -1; dy <= 1; ++dy) {
-        for (int dx = -1; dx <= 1; ++dx) {
-          const int ncx = c.x + dx, ncy = c.y + dy;
-          const uint32_t h = hs[3 * (dy + 1) + (dx + 1)];
-          const uint32_t e0 = S.bucketStart[h], e1 = S.bucketStart[h + 1];
-          for (uint32_t e = e0; e < e1; ++e) {
-            const uint32_t j = S.grid[e];
-            if (j == i) continue;
-            const int2 cj = S.cellXY[j];
-            if (cj.x != ncx || cj.y != ncy || S.segOf[j] != sg) continue;
-            if (boxes_overlap(bi, i, S.box[j], j)) {
-              if (cnt < kStash) stash[cnt] = j;
-              ++cnt;
-            }
-          }
-        }
-      }
+      for_each_cell_neighbour(S, i, sg, bi, mask, [&](uint32_t j) {
+        if (cnt < kStash) stash[cnt] = j;
+        ++cnt;
+      });
       for (uint32_t k = 0; k < lCount; ++k) {
         const uint32_t j = S.largeList[lStart + k];
         if (boxes_overlap(bi, i, S.box[j], j)) {
@@ -335,23 +354,8 @@ __global__ void __launch_bounds__(kBlock)
       for (uint32_t a = 0; a < cnt; ++a) S.plist[base + a] = stash[a];
     } else {
       uint32_t w = 0;
-      const int2 c = S.cellXY[i];
-      uint32_t hs[9];
-      cell_hash3x3(sg, c.x, c.y, mask, hs);
-      for (int dy = -1; dy <= 1; ++dy) {
-        for (int dx = -1; dx <= 1; ++dx) {
-          const int ncx = c.x + dx, ncy = c.y + dy;
-          const uint32_t h = hs[3 * (dy + 1) + (dx + 1)];
-          const uint32_t e0 = S.bucketStart[h], e1 = S.bucketStart[h + 1];
-          for (uint32_t e = e0; e < e1; ++e) {
-            const uint32_t j = S.grid[e];
-            if (j == i) continue;
-            const int2 cj = S.cellXY[j];
-            if (cj.x != ncx || cj.y != ncy || S.segOf[j] != sg) continue;
-            if (boxes_overlap(bi, i, S.box[j], j)) S.plist[base + w++] = j;
-          }
-        }
-      }
+      for_each_cell_neighbour(S, i, sg, bi, mask,
+                              [&](uint32_t j) { S.plist[base + w++] = j; });
       for (uint32_t k = 0; k < lCount; ++k) {
         const uint32_t j = S.largeList[lStart + k];
         if (boxes_overlap(bi, i, S.box[j], j)) S.plist[base + w++] = j;
