@@ -256,28 +256,55 @@ __global__ void __launch_bounds__(kSortThreads, 3)
     rank[k] = b + before;
   }
   __syncthreads();
-  // per-digit: warp-exclusive prefixes and the tile count
+  // per digit (one per thread): warp-exclusive prefixes and the tile count,
+  // published at once so that successors can look past this tile while it
+  // orders its items
+  const int d = tid; // kSortThreads == 256
+  uint32_t count = 0;
   {
-    const int d = tid; // kSortThreads == 256
-    uint32_t run = 0;
 #pragma unroll
     for (int w = 0; w < kSortWarps; ++w) {
       const uint32_t c = s_whist[w][d];
-      s_whist[w][d] = run;
-      run += c;
+      s_whist[w][d] = count;
+      count += c;
     }
-    const uint32_t count = run;
-    // look-back for this digit
+    st_relaxed_u32(status + (size_t)tile * 256 + d,
+                   ((tile == 0 ? 2u : 1u) << kRFlagShift) | count);
+  }
+  // exclusive scan of tile counts over digits (256 entries, one per thread)
+  {
+    uint32_t inc = count;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    __shared__ uint32_t s_wsum[kSortWarps];
+    if (lane == 31) s_wsum[warp] = inc;
+    __syncthreads();
+    uint32_t off = 0;
+    for (int w = 0; w < warp; ++w) off += s_wsum[w];
+    s_local[tid] = off + inc - count;
+  }
+  __syncthreads();
+  // local reorder by digit (stable)
+#pragma unroll
+  for (int k = 0; k < kSortItems; ++k) {
+    const uint32_t dk = dig[k];
+    if (dk < 256u) {
+      const uint32_t p = s_local[dk] + s_whist[warp][dk] + rank[k];
+      s_keys[p] = key[k];
+      s_vals[p] = val[k];
+    }
+  }
+  // look-back for digit d, with the items already out of registers
+  {
     uint32_t excl = 0;
-    uint32_t *my = status + (size_t)tile * 256 + d;
-    if (tile == 0) {
-      st_relaxed_u32(my, (2u << kRFlagShift) | count);
-    } else {
-      st_relaxed_u32(my, (1u << kRFlagShift) | count);
-      // look back over kLookBack predecessors per round trip (independent
-      // loads in flight); tile 0 is always inclusive, so the walk ends
-      // before it would read below tile 0
-      constexpr int kLookBack = 8;
+    if (tile != 0) {
+      // kLookBack predecessors per round trip (independent loads in
+      // flight); tile 0 is always inclusive, so the walk ends before it
+      // would read below tile 0
+      constexpr int kLookBack = 16;
       int pred = (int)tile - 1;
       uint32_t spins = 0;
       for (;;) {
@@ -307,46 +334,17 @@ __global__ void __launch_bounds__(kSortThreads, 3)
           __nanosleep(32);
         }
       }
-      st_relaxed_u32(my, (2u << kRFlagShift) | ((excl + count) & kRValueMask));
+      st_relaxed_u32(status + (size_t)tile * 256 + d,
+                     (2u << kRFlagShift) | ((excl + count) & kRValueMask));
     }
     s_global[d] = digitStart[d] + excl;
-    s_local[d] = count;
-  }
-  __syncthreads();
-  // exclusive scan of tile counts over digits (256 entries, one per thread)
-  {
-    const uint32_t c = s_local[tid];
-    uint32_t inc = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
-      if (lane >= o) inc += t;
-    }
-    __shared__ uint32_t s_wsum[kSortWarps];
-    if (lane == 31) s_wsum[warp] = inc;
-    __syncthreads();
-    uint32_t off = 0;
-    for (int w = 0; w < warp; ++w) off += s_wsum[w];
-    __syncthreads();
-    s_local[tid] = off + inc - c;
-  }
-  __syncthreads();
-  // local reorder by digit (stable)
-#pragma unroll
-  for (int k = 0; k < kSortItems; ++k) {
-    const uint32_t d = dig[k];
-    if (d < 256u) {
-      const uint32_t p = s_local[d] + s_whist[warp][d] + rank[k];
-      s_keys[p] = key[k];
-      s_vals[p] = val[k];
-    }
   }
   __syncthreads();
   const uint32_t valid = min((uint32_t)kSortTile, n - base);
   for (uint32_t p = tid; p < valid; p += kSortThreads) {
     const K k = s_keys[p];
-    const uint32_t d = (uint32_t)((k >> shift) & 255u);
-    const uint32_t dest = s_global[d] + (p - s_local[d]);
+    const uint32_t dk = (uint32_t)((k >> shift) & 255u);
+    const uint32_t dest = s_global[dk] + (p - s_local[dk]);
     keysOut[dest] = k;
     valsOut[dest] = s_vals[p];
   }
