@@ -135,6 +135,17 @@ int nbx_download_bodies(nbx_handle *h, nbx_body *bodies, size_t n,
  * per step and returns; errors raised on the device surface at nbx_sync. */
 int nbx_step(nbx_handle *h, uint32_t steps);
 
+/* One Simulation::step() on host-owned bodies, the call the drop-in
+ * Simulation::step() makes (Simulation.cpp:11-16 over the caller's
+ * vector): uploads `in` (as nbx_upload_bodies), steps once and writes the
+ * bodies in their order after the step (as nbx_download_bodies with
+ * id_order 0) to `out`; synchronous.  in may equal out.  When out is
+ * pinned host memory the force pass runs in ranges and each range's
+ * records are copied to out while the later ranges still compute, so most
+ * of the device-to-host copy is hidden; otherwise it is upload, step,
+ * download. */
+int nbx_step_io(nbx_handle *h, const nbx_body *in, nbx_body *out, size_t n);
+
 /* The viewer's attractor (CudaSimulation.cuh:9-15, attractorKernel
  * CudaSimulation.cu:14-31): while active, every step adds to each body's
  * acceleration the pull of a point mass at (x, y),

@@ -126,8 +126,8 @@ __global__ void k_frame_scatter(const float4 *__restrict__ pv,
 __global__ void k_pack(const float4 *__restrict__ pv, const float2 *__restrict__ acc,
                        const float2 *__restrict__ mr, const uint32_t *__restrict__ id,
                        const uint16_t *__restrict__ segOf, const SegDev *seg,
-                       uint32_t n, int idOrder, nbx_body *out) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+                       uint32_t begin, uint32_t n, int idOrder, nbx_body *out) {
+  for (uint32_t i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += gridDim.x * blockDim.x) {
     const float4 p = pv[i];
     const float2 a = acc[i];
@@ -242,6 +242,16 @@ struct nbx_handle {
   uint32_t timedSteps = 0;                        // steps of the last call
   bool timedValid = false;
   bool timedCapture = false;
+  // step graphs of nbx_step_io: the force pass in kIoChunks target ranges
+  // on their own streams, each range packed and copied to ioOut (pinned
+  // host memory) as soon as its forces are done
+  static constexpr int kIoChunks = 8;
+  cudaGraphExec_t ioGraph[2] = {nullptr, nullptr};
+  nbx_body *ioOut = nullptr;   // the host buffer the io graphs write
+  bool ioCapture = false;
+  cudaStream_t ioStream[kIoChunks] = {};
+  cudaEvent_t ioFork = nullptr;
+  cudaEvent_t ioDone[kIoChunks] = {};
   bool uploaded = false;
   bool treeValid = false;   // a Barnes-Hut tree of the current state exists
   bool bfsValid = false;    // its breadth-first arrays (built on demand)
@@ -361,6 +371,7 @@ int allocate(nbx_handle *h) {
   A(S.bucketCount, S.nBuckets + 1);
   A(S.bucketStart, S.nBuckets + 2);
   A(S.grid, n);
+  A(S.gridBox, n);
   A(S.largeCount, ns);
   A(S.largeStartA, ns + 1);
   A(S.largeList, n);
@@ -484,6 +495,42 @@ bool forces_unclamped(const nbx_handle *h) {
          h->maxMass < 1.6e19f * fminf(1.0f, eSq);
 }
 
+// Ranges of the force pass for nbx_step_io: whole warps, at most
+// kIoChunks of them, none for fewer than 64K bodies (the copy is short).
+uint32_t io_chunks(const nbx_handle *h) {
+  const uint32_t c = h->n / 65536u;
+  return c < 1u ? 1u : (c > (uint32_t)nbx_handle::kIoChunks ? (uint32_t)nbx_handle::kIoChunks : c);
+}
+
+// The force pass of an io step graph: each target range on its own stream
+// (forked from s after the build, so the ranges run as one pool of blocks,
+// dispatched in range order), writing its bodies' whole records; each
+// range's records go to the host as soon as its launch ends, while the
+// later ranges still compute.  s joins every range.
+static_assert(sizeof(nbx_body) == 9 * sizeof(uint32_t), "the force pass writes 9-word records");
+void enqueue_forces_io(nbx_handle *h, cudaStream_t s, const DevState &S) {
+  const uint32_t n = S.n, chunks = io_chunks(h);
+  const uint32_t per = ((n + chunks - 1) / chunks + 31u) & ~31u;
+  cudaEventRecord(h->ioFork, s);
+  for (uint32_t c = 0; c < chunks; ++c) {
+    const uint32_t b = c * per, e = std::min(n, b + per);
+    if (b >= e) break;
+    cudaStream_t cs = h->ioStream[c];
+    cudaStreamWaitEvent(cs, h->ioFork, 0);
+    DevState R = S;
+    R.forceBegin = b;
+    R.forceEnd = e;
+    R.recOut = reinterpret_cast<uint32_t *>(h->dAoS);
+    launch_forces(cs, R, h->params.exact_math != 0, h->params.force_blocks,
+                  h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band, h->params.use_mlp,
+                  forces_unclamped(h), h->params.force_block, h->params.leaf_pairs != 0);
+    cudaMemcpyAsync(h->ioOut + b, h->dAoS + b, (size_t)(e - b) * sizeof(nbx_body),
+                    cudaMemcpyDeviceToHost, cs);
+    cudaEventRecord(h->ioDone[c], cs);
+    cudaStreamWaitEvent(s, h->ioDone[c], 0);
+  }
+}
+
 // One Simulation::step on stream s for state S; returns the state after the
 // Morton gather's buffer swap.
 DevState enqueue_step(nbx_handle *h, cudaStream_t s, DevState S) {
@@ -505,6 +552,10 @@ DevState enqueue_step(nbx_handle *h, cudaStream_t s, DevState S) {
   }
   // second moments only where the force pass reads them
   launch_build(s, S, h->scan, h->sort, h->params.use_mlp != 0);
+  if (h->ioCapture) {
+    enqueue_forces_io(h, s, S);
+    return S;
+  }
   if (h->timedCapture) cudaEventRecordWithFlags(h->forceMark[0], s, cudaEventRecordExternal);
   launch_forces(s, S, h->params.exact_math != 0, h->params.force_blocks,
                 h->mlpLoaded ? h->mlpW : nullptr, h->params.mlp_band,
@@ -528,6 +579,11 @@ void destroy_graphs(nbx_handle *h) {
     h->graphTSrc[p] = nullptr;
   }
   h->timedValid = false;
+  for (auto &g : h->ioGraph) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+  h->ioOut = nullptr;
 }
 
 // Flags after a whole step: the naive law builds no tree.
@@ -614,6 +670,51 @@ int capture_graphs(nbx_handle *h) {
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
   }
   h->graphsValid = true;
+  return NBX_OK;
+}
+
+// The two io step graphs writing to out (pinned host memory).
+int capture_io_graphs(nbx_handle *h, nbx_body *out) {
+  for (auto &g : h->ioGraph) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+  h->ioOut = nullptr;
+  if (!h->ioFork) {
+    NBX_CUDA(h, cudaEventCreateWithFlags(&h->ioFork, cudaEventDisableTiming));
+    // earlier ranges on higher-priority streams: their blocks are
+    // dispatched first, so the ranges finish (and copy) in order
+    int least = 0, greatest = 0;
+    NBX_CUDA(h, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    for (int c = 0; c < nbx_handle::kIoChunks; ++c) {
+      const int prio = std::min(greatest + c, least);
+      NBX_CUDA(h, cudaStreamCreateWithPriority(&h->ioStream[c], cudaStreamNonBlocking, prio));
+      NBX_CUDA(h, cudaEventCreateWithFlags(&h->ioDone[c], cudaEventDisableTiming));
+    }
+  }
+  h->ioOut = out;
+  for (int p = 0; p < 2; ++p) {
+    const int saved = h->cur;
+    h->cur = p;
+    const DevState S = h->state();
+    h->cur = saved;
+    cudaGraph_t g = nullptr;
+    NBX_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    h->ioCapture = true;
+    enqueue_step(h, h->stream, S);
+    h->ioCapture = false;
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (e != cudaSuccess) {
+      h->ioOut = nullptr;
+      return cuda_fail(h, e, "cudaStreamEndCapture");
+    }
+    e = cudaGraphInstantiate(&h->ioGraph[p], g, cudaGraphInstantiateFlagUseNodePriority);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      h->ioOut = nullptr;
+      return cuda_fail(h, e, "cudaGraphInstantiate");
+    }
+  }
   return NBX_OK;
 }
 
@@ -728,6 +829,11 @@ int nbx_destroy(nbx_handle *h) {
   for (cudaEvent_t ev : h->forceEv) cudaEventDestroy(ev);
   for (cudaEvent_t ev : h->forceMark)
     if (ev) cudaEventDestroy(ev);
+  if (h->ioFork) cudaEventDestroy(h->ioFork);
+  for (int c = 0; c < nbx_handle::kIoChunks; ++c) {
+    if (h->ioDone[c]) cudaEventDestroy(h->ioDone[c]);
+    if (h->ioStream[c]) cudaStreamDestroy(h->ioStream[c]);
+  }
   for (void *v : h->allocs) cudaFree(v);
   for (void *v : h->scratch) cudaFree(v);
   if (h->hPinned) cudaFreeHost(h->hPinned);
@@ -868,7 +974,7 @@ int nbx_download_bodies(nbx_handle *h, nbx_body *bodies, size_t n, int idOrder) 
   if (n == 0) return NBX_OK;
   const DevState S = h->state();
   k_pack<<<std::min<uint32_t>((h->n + 255) / 256, 4096), 256, 0, h->stream>>>(
-      S.pv, S.acc, S.mr, S.id, S.segOf, S.seg, h->n, idOrder, h->dAoS);
+      S.pv, S.acc, S.mr, S.id, S.segOf, S.seg, 0u, h->n, idOrder, h->dAoS);
   NBX_CUDA(h, cudaGetLastError());
   cudaPointerAttributes attr{};
   const bool pinned = cudaPointerGetAttributes(&attr, bodies) == cudaSuccess &&
@@ -899,6 +1005,37 @@ int nbx_step(nbx_handle *h, uint32_t steps) {
   }
   after_step(h);
   return NBX_OK;
+}
+
+int nbx_step_io(nbx_handle *h, const nbx_body *in, nbx_body *out, size_t n) {
+  if (!h || (!in && n) || (!out && n) || n != h->n)
+    return h ? fail(h, NBX_ERR_ARG, "body count mismatch") : NBX_ERR_ARG;
+  int rc = nbx_upload_bodies(h, in, n);
+  if (rc != NBX_OK || n == 0) return rc;
+  if (h->params.use_mlp == 1 && !h->mlpLoaded)
+    return fail(h, NBX_ERR_STATE, "use_mlp = 1 without MLP parameters");
+  cudaPointerAttributes attr{};
+  const bool pinned = cudaPointerGetAttributes(&attr, out) == cudaSuccess &&
+                      attr.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  if (!pinned || h->params.force_law != 0) {
+    // pageable memory cannot be a graph's copy target: step, then copy
+    rc = nbx_step(h, 1);
+    if (rc != NBX_OK) return rc;
+    return nbx_download_bodies(h, out, n, 0);
+  }
+  if (!h->graphsValid) {
+    rc = capture_graphs(h);
+    if (rc != NBX_OK) return rc;
+  }
+  if (h->ioOut != out || !h->ioGraph[h->cur]) {
+    rc = capture_io_graphs(h, out);
+    if (rc != NBX_OK) return rc;
+  }
+  NBX_CUDA(h, cudaGraphLaunch(h->ioGraph[h->cur], h->stream));
+  h->cur ^= 1;
+  after_step(h);
+  return check_status(h);
 }
 
 int nbx_step_timed(nbx_handle *h, uint32_t steps) {

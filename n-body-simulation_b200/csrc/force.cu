@@ -366,9 +366,11 @@ __device__ __forceinline__ void forces_walk(
   const int lane = threadIdx.x & 31;
   const int w = threadIdx.x >> 5;
   const uint32_t warpsTotal = (gridDim.x * blockDim.x) >> 5;
-  // query points (instance 0's tree) instead of the bodies, if given
-  const uint32_t nTargets = query ? nQuery : S.n;
-  for (uint32_t wb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+  // query points (instance 0's tree) instead of the bodies, if given; for
+  // the bodies, the launch's range of targets
+  const uint32_t tBegin = query ? 0u : S.forceBegin;
+  const uint32_t nTargets = query ? nQuery : (S.forceEnd ? min(S.forceEnd, S.n) : S.n);
+  for (uint32_t wb = tBegin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
        wb < nTargets; wb += warpsTotal * 32) {
     const uint32_t i = wb + lane;
     const bool valid = i < nTargets;
@@ -426,6 +428,22 @@ __device__ __forceinline__ void forces_walk(
       } else {
         add_attractor<kExact>(S.attr, x, y, ax, ay);
         S.acc[i] = make_float2(ax, ay);
+        if (S.recOut) {
+          // the body's whole record (nbx_body: pos, vel, acc, mass,
+          // radius, id), for a copy to the host right after this launch
+          const float4 p = S.pv[i];
+          const float2 m = S.mr[i];
+          uint32_t *r = S.recOut + (size_t)i * 9;
+          r[0] = __float_as_uint(p.x);
+          r[1] = __float_as_uint(p.y);
+          r[2] = __float_as_uint(p.z);
+          r[3] = __float_as_uint(p.w);
+          r[4] = __float_as_uint(ax);
+          r[5] = __float_as_uint(ay);
+          r[6] = __float_as_uint(m.x);
+          r[7] = __float_as_uint(m.y);
+          r[8] = S.id[i];
+        }
       }
     }
   }
@@ -529,12 +547,18 @@ void launch_query_forces(cudaStream_t s, const DevState &S, bool exact,
                                                       nq, out);
 }
 
+// Bodies a force launch over S covers (its target range, or all).
+uint32_t force_targets(const DevState &S) {
+  const uint32_t e = S.forceEnd ? (S.forceEnd < S.n ? S.forceEnd : S.n) : S.n;
+  return e > S.forceBegin ? e - S.forceBegin : 0u;
+}
+
 // The default plain walk with kBlock threads per block and the paired or
 // single-body leaf loop.
 template <int kBlock>
 void launch_plain(cudaStream_t s, const DevState &S, int blocks, bool pairs) {
   if (blocks <= 0) {
-    const uint32_t warps = (S.n + 31) / 32, per = kBlock / 32;
+    const uint32_t warps = (force_targets(S) + 31) / 32, per = kBlock / 32;
     const uint32_t b = (warps + per - 1) / per;
     blocks = (int)(b ? b : 1);
   }
@@ -554,7 +578,7 @@ void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
     return;
   }
   if (blocks <= 0) {
-    uint32_t warps = (S.n + 31) / 32;
+    uint32_t warps = (force_targets(S) + 31) / 32;
     uint32_t b = (warps + kWarps - 1) / kWarps;
     blocks = (int)(b ? b : 1);
   }

@@ -58,6 +58,12 @@ struct DevState {
   float dt, tSq, eSq;
   int leafCapacity;
   int collisions;
+  // force targets [forceBegin, forceEnd) of a force launch; forceEnd 0:
+  // every body (the step graphs of nbx_step_io split the pass in ranges)
+  uint32_t forceBegin, forceEnd;
+  // with recOut, the force pass also writes each target's 9-word body
+  // record (the nbx_body layout) there
+  uint32_t *recOut;
 
   SegDev *seg;
   uint16_t *segOf; // segment of each body index (never permuted)
@@ -83,6 +89,7 @@ struct DevState {
   uint32_t *bucketCount; // [buckets]
   uint32_t *bucketStart; // [buckets+1]
   uint32_t *grid;        // body index per bucket slot
+  float4 *gridBox;       // the box of that body (read with the index)
   uint32_t nBuckets;     // power of two
   uint32_t *largeCount;  // [nseg]
   uint32_t *largeStartA; // [nseg]

@@ -135,10 +135,8 @@ void Simulation::step() {
   if (!bodies.empty()) {
     ctx_->ensure(bodies.size(), params_for(dt, quadtree.theta(), quadtree.epsilon(),
                                            quadtree.leafCapacity()));
-    ctx_->upload(bodies);
-    ctx_->check(nbx_step(ctx_->h, 1), "nbx_step");
-    ctx_->check(nbx_sync(ctx_->h), "nbx_sync");
-    ctx_->download(bodies);
+    nbx_body *b = reinterpret_cast<nbx_body *>(bodies.data());
+    ctx_->check(nbx_step_io(ctx_->h, b, b, bodies.size()), "nbx_step_io");
   }
   frame += 1;
 }

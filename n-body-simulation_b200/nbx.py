@@ -28,6 +28,7 @@ assert BODY_DTYPE.itemsize == 36
 EXPORTS = (
     "nbx_params_default", "nbx_create", "nbx_destroy", "nbx_set_params",
     "nbx_get_params", "nbx_upload_bodies", "nbx_download_bodies", "nbx_step",
+    "nbx_step_io",
     "nbx_sync", "nbx_phase", "nbx_get_morton", "nbx_tree_size", "nbx_get_tree",
     "nbx_get_pairs", "nbx_direct_fp64", "nbx_force_error_fp64",
     "nbx_energy_momentum_fp64", "nbx_status_bits", "nbx_last_error",
@@ -110,6 +111,7 @@ def lib() -> C.CDLL:
         "nbx_upload_bodies": [vp, vp, C.c_size_t],
         "nbx_download_bodies": [vp, vp, C.c_size_t, C.c_int],
         "nbx_step": [vp, C.c_uint32],
+        "nbx_step_io": [vp, vp, vp, C.c_size_t],
         "nbx_step_timed": [vp, C.c_uint32],
         "nbx_force_times": [vp, vp, C.c_uint32],
         "nbx_make_scenario": [C.c_int, C.c_uint32, C.c_uint32, vp],
@@ -348,6 +350,17 @@ class Handle:
 
     def download_ptr(self, ptr: int, n: int, id_order: bool = False):
         self._c(lib().nbx_download_bodies(self.h, ptr, n, int(id_order)))
+
+    def step_io(self, bodies: np.ndarray, out: np.ndarray | None = None):
+        """One step on host bodies (upload, step, download in the bodies'
+        order after the step); out may be bodies itself."""
+        if out is None:
+            out = np.empty(self.n, BODY_DTYPE)
+        self._c(lib().nbx_step_io(self.h, bodies.ctypes.data, out.ctypes.data, self.n))
+        return out
+
+    def step_io_ptr(self, ptr_in: int, ptr_out: int, n: int):
+        self._c(lib().nbx_step_io(self.h, ptr_in, ptr_out, n))
 
     def step(self, steps: int = 1):
         self._c(lib().nbx_step(self.h, steps))

@@ -241,6 +241,43 @@ def test_step_timed_same_state(nbx):
     t.close()
 
 
+@pytest.mark.parametrize("n", [1000, 65536 + 17, 300001])
+def test_step_io_equals_upload_step_download(nbx, n):
+    """nbx_step_io (the drop-in Simulation::step on host bodies) gives the
+    bodies that upload + step + download give, bit for bit: into pinned
+    memory (force ranges copied while later ranges compute; 1, 1 and 4
+    ranges at these sizes), into pageable memory, in place, and after a
+    parameter change (new graphs)."""
+    import torch
+
+    b = nbx.two_discs(n, 0, 0.2)
+    ref = nbx.Simulation(b, theta=0.5)
+    cur = b.copy()
+    expect = []
+    for k in range(4):
+        if k == 2:
+            ref.set_params(theta=0.7)
+        ref.upload(cur)
+        ref.step(1)
+        cur = ref.download()
+        expect.append(cur)
+    ref.close()
+    pinned = torch.empty(n * 36, dtype=torch.uint8, pin_memory=True)
+    hb = pinned.numpy().view(nbx.BODY_DTYPE)
+    sim = nbx.Simulation(b, theta=0.5)
+    hb[:] = b
+    for k in range(4):
+        if k == 2:
+            sim.set_params(theta=0.7)
+        if k == 1:  # pageable in, pageable out
+            out = sim.step_io(hb.copy())
+            hb[:] = out
+        else:  # pinned, in place
+            sim.step_io_ptr(pinned.data_ptr(), pinned.data_ptr(), n)
+        assert same_bits(hb, expect[k]), k
+    sim.close()
+
+
 def test_deterministic(nbx):
     b = nbx.uniform_disc(20000)
     outs = []
