@@ -5,6 +5,7 @@
 #include "nbx_state.cuh"
 
 #include <algorithm>
+#include <cstddef>
 #include <cfloat>
 #include <cmath>
 #include <condition_variable>
@@ -262,6 +263,9 @@ struct nbx_handle {
   bool idsPermutation = false;
   nbx_body *dAoS = nullptr;     // device staging of body records
   nbx_body *hPinned = nullptr;  // pinned host staging
+  // pinned words for the upload's small copies: [0] largest mass bits,
+  // [1] coordinate limit bits, [4 + 3 s ..] instance s's collision cell
+  uint32_t *hWord = nullptr;
   double2 *dPartial = nullptr;  // FP64 direct-sum partials
   uint32_t dPartialTargets = 0;
   double *dF64 = nullptr;       // small FP64 scratch
@@ -468,6 +472,7 @@ int allocate(nbx_handle *h) {
   }
   NBX_CUDA(h, cudaStreamSynchronize(h->stream));
   NBX_CUDA(h, cudaMallocHost(&h->hPinned, std::max<size_t>(n, 1) * sizeof(nbx_body)));
+  NBX_CUDA(h, cudaMallocHost(&h->hWord, (4 + 3 * (size_t)ns) * sizeof(uint32_t)));
   return NBX_OK;
 }
 
@@ -837,6 +842,7 @@ int nbx_destroy(nbx_handle *h) {
   for (void *v : h->allocs) cudaFree(v);
   for (void *v : h->scratch) cudaFree(v);
   if (h->hPinned) cudaFreeHost(h->hPinned);
+  if (h->hWord) cudaFreeHost(h->hWord);
   if (h->dPartial) cudaFree(h->dPartial);
   if (h->dTargets) cudaFree(h->dTargets);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -884,14 +890,34 @@ int nbx_upload_bodies(nbx_handle *h, const nbx_body *bodies, size_t n) {
   k_unpack<<<std::min<uint32_t>((h->n + 255) / 256, 4096), 256, 0, h->stream>>>(
       h->dAoS, h->n, S.pv, S.acc, S.mr, S.id, S.counters + 12);
   NBX_CUDA(h, cudaGetLastError());
-  uint32_t massBits = 0;
-  NBX_CUDA(h, cudaMemcpyAsync(&massBits, S.counters + 12, sizeof(uint32_t),
+  NBX_CUDA(h, cudaMemcpyAsync(h->hWord, S.counters + 12, sizeof(uint32_t),
                               cudaMemcpyDeviceToHost, h->stream));
-  // collision cell per instance: 2 x median radius x 1.01 (CudaCollision.cu:201-215)
-  std::vector<SegDev> seg(h->nseg);
-  NBX_CUDA(h, cudaMemcpyAsync(seg.data(), S.seg, h->nseg * sizeof(SegDev),
-                              cudaMemcpyDeviceToHost, h->stream));
+  // While the records cross PCIe: the collision cell per instance, 2 x
+  // 1.01 x the median radius (CudaCollision.cu:201-215).  The cell only
+  // sets how the broadphase partitions space: the candidate set (every
+  // overlapping box pair) does not depend on it.  The median is over an
+  // evenly strided sample of at most 4096 bodies per instance (the
+  // reference takes all radii); deterministic for a given input.
+  std::vector<float> cells(3 * (size_t)h->nseg); // {cell, invCell, smallW}
+  std::vector<float> radii;
+  for (uint32_t s = 0; s < h->nseg; ++s) {
+    const uint32_t s0 = h->segStart[s], cnt = h->segCount[s];
+    const uint32_t stride = cnt > 4096 ? cnt / 4096 : 1;
+    radii.clear();
+    for (uint32_t i = 0; i < cnt; i += stride) radii.push_back(bodies[s0 + i].radius);
+    float cell = 1.0f;
+    if (!radii.empty()) {
+      const size_t mid = radii.size() / 2;
+      std::nth_element(radii.begin(), radii.begin() + mid, radii.end());
+      cell = 2.0f * radii[mid] * 1.01f;
+    }
+    if (!(cell > 0.0f) || !std::isfinite(cell)) cell = 1.0f;
+    cells[3 * s] = cell;
+    cells[3 * s + 1] = 1.0f / cell;
+    cells[3 * s + 2] = cell * 0.999f;
+  }
   NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  const uint32_t massBits = *h->hWord;
   // the force pass leaves out its FLT_MAX clamp when it cannot act; a
   // change of that choice needs new step graphs
   uint32_t coordLimitBits = 0;
@@ -908,33 +934,20 @@ int nbx_upload_bodies(nbx_handle *h, const nbx_body *bodies, size_t n) {
       lim = std::fmin(lim, 1e36f / (static_cast<float>(h->n) * mm));
     std::memcpy(&coordLimitBits, &lim, sizeof(lim));
   }
-  // The grid cell only sets how the broadphase partitions space: the
-  // candidate set (every overlapping box pair) does not depend on it.  It
-  // is 2 x 1.01 x the median radius of an evenly strided sample of at most
-  // 4096 bodies per instance (CudaCollision.cu:201-215 takes the median of
-  // all radii); deterministic for a given input.
-  std::vector<float> radii;
-  for (uint32_t s = 0; s < h->nseg; ++s) {
-    const uint32_t s0 = h->segStart[s], cnt = h->segCount[s];
-    const uint32_t stride = cnt > 4096 ? cnt / 4096 : 1;
-    radii.clear();
-    for (uint32_t i = 0; i < cnt; i += stride) radii.push_back(bodies[s0 + i].radius);
-    float cell = 1.0f;
-    if (!radii.empty()) {
-      const size_t mid = radii.size() / 2;
-      std::nth_element(radii.begin(), radii.begin() + mid, radii.end());
-      cell = 2.0f * radii[mid] * 1.01f;
-    }
-    if (!(cell > 0.0f) || !std::isfinite(cell)) cell = 1.0f;
-    seg[s].cell = cell;
-    seg[s].invCell = 1.0f / cell;
-    seg[s].smallW = cell * 0.999f;
-  }
-  NBX_CUDA(h, cudaMemcpyAsync(S.seg, seg.data(), h->nseg * sizeof(SegDev),
-                              cudaMemcpyHostToDevice, h->stream));
-  NBX_CUDA(h, cudaMemcpyAsync(S.counters + kCtrCoordLimit, &coordLimitBits,
-                              sizeof(coordLimitBits), cudaMemcpyHostToDevice, h->stream));
-  NBX_CUDA(h, cudaStreamSynchronize(h->stream));
+  // the three cell fields of every SegDev and the limit, ordered before
+  // the next step on the stream; the pinned words are free again once the
+  // synchronisation above has passed (the last upload's copies came before)
+  h->hWord[1] = coordLimitBits;
+  std::memcpy(h->hWord + 4, cells.data(), cells.size() * sizeof(float));
+  static_assert(offsetof(SegDev, invCell) == offsetof(SegDev, cell) + 4 &&
+                    offsetof(SegDev, smallW) == offsetof(SegDev, cell) + 8,
+                "SegDev cell fields are contiguous");
+  NBX_CUDA(h, cudaMemcpy2DAsync(reinterpret_cast<char *>(S.seg) + offsetof(SegDev, cell),
+                                sizeof(SegDev), h->hWord + 4, 3 * sizeof(float),
+                                3 * sizeof(float), h->nseg, cudaMemcpyHostToDevice,
+                                h->stream));
+  NBX_CUDA(h, cudaMemcpyAsync(S.counters + kCtrCoordLimit, h->hWord + 1,
+                              sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
   h->idsChecked = false;
   h->uploaded = true;
   h->treeValid = false;
