@@ -29,6 +29,7 @@ void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
                   SortScratch &sort, bool moments);
 void launch_bfs_tree(cudaStream_t s, const DevState &S, ScanScratch &scan,
                      SortScratch &sort);
+void launch_step_zero(cudaStream_t s, const DevState &S, SortScratch &sort, bool grid);
 void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
                    const MlpDev *mlp, float band, int corr, bool noClamp, int threads,
                    bool pairs);
@@ -539,10 +540,7 @@ void enqueue_forces_io(nbx_handle *h, cudaStream_t s, const DevState &S) {
 // One Simulation::step on stream s for state S; returns the state after the
 // Morton gather's buffer swap.
 DevState enqueue_step(nbx_handle *h, cudaStream_t s, DevState S) {
-  if (S.collisions) {
-    cudaMemsetAsync(S.bucketCount, 0, sizeof(uint32_t) * (S.nBuckets + 1), s);
-    cudaMemsetAsync(S.largeCount, 0, sizeof(uint32_t) * S.nseg, s);
-  }
+  launch_step_zero(s, S, h->sort, S.collisions != 0);
   launch_integrate(s, S, true, S.collisions != 0);
   mark(s, "integrate");
   if (S.collisions) launch_collide(s, S, h->scan, h->sort);
@@ -1431,8 +1429,7 @@ int nbx_phase(nbx_handle *h, int phase) {
     launch_integrate(s, S, true, false);
     break;
   case NBX_PHASE_COLLIDE:
-    cudaMemsetAsync(S.bucketCount, 0, sizeof(uint32_t) * (S.nBuckets + 1), s);
-    cudaMemsetAsync(S.largeCount, 0, sizeof(uint32_t) * S.nseg, s);
+    launch_step_zero(s, S, h->sort, true);
     launch_integrate(s, S, false, true);
     launch_collide(s, S, h->scan, h->sort);
     h->collideValid = true;
@@ -1445,6 +1442,7 @@ int nbx_phase(nbx_handle *h, int phase) {
       h->forceInput = true;
       break;
     }
+    launch_step_zero(s, S, h->sort, false);
     launch_build(s, S, h->scan, h->sort, true);
     h->momentsValid = true;
     h->cur ^= 1;
@@ -1473,6 +1471,7 @@ int nbx_phase(nbx_handle *h, int phase) {
       launch_naive_forces(s, S, h->params.exact_math != 0);
       break;
     }
+    launch_step_zero(s, S, h->sort, false);
     launch_build(s, S, h->scan, h->sort, true);
     h->momentsValid = true;
     h->cur ^= 1;

@@ -41,40 +41,6 @@ int grid_for(uint32_t n) {
   return b ? (int)b : 1;
 }
 
-__device__ __forceinline__ float key_to_float(uint32_t k) {
-  return u2f((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
-}
-
-// Root square per instance (Quad::newContaining, QuadTree.cpp:30-51, and
-// rootSquare, CudaQuadTree.cu:25-30) and the Morton frame.  Resets the
-// bound accumulators for the next step.
-__global__ void k_root_frame(DevState S) {
-  const uint32_t sg = blockIdx.x * blockDim.x + threadIdx.x;
-  if (sg >= S.nseg) return;
-  uint32_t *b = S.bounds + 4 * sg;
-  const float minX = b[0] == 0xffffffffu ? FLT_MAX : key_to_float(b[0]);
-  const float maxX = b[1] == 0u ? -FLT_MAX : key_to_float(b[1]);
-  const float minY = b[2] == 0xffffffffu ? FLT_MAX : key_to_float(b[2]);
-  const float maxY = b[3] == 0u ? -FLT_MAX : key_to_float(b[3]);
-  const float cx = __fmul_rn(__fadd_rn(minX, maxX), 0.5f);
-  const float cy = __fmul_rn(__fadd_rn(minY, maxY), 0.5f);
-  const float w = __fsub_rn(maxX, minX), h = __fsub_rn(maxY, minY);
-  const float size = (w < h) ? h : w;
-  SegDev &G = S.seg[sg];
-  G.cx = cx;
-  G.cy = cy;
-  G.size = size;
-  G.frame = sd_morton_frame(cx, cy, size);
-  // clamp guard: bodies beyond the upload's coordinate limit (NaN-safe)
-  const float lim = __uint_as_float(S.counters[kCtrCoordLimit]);
-  const float reach = fmaxf(fmaxf(fabsf(minX), fabsf(maxX)), fmaxf(fabsf(minY), fabsf(maxY)));
-  G.wide = (b[0] != 0xffffffffu && !(reach < lim)) ? 1u : 0u;
-  b[0] = 0xffffffffu;
-  b[1] = 0u;
-  b[2] = 0xffffffffu;
-  b[3] = 0u;
-}
-
 // quantise() in native FP64 (TreeKernels.cuh:48-57): one IEEE subtract and
 // one multiply, each rounded (no contraction), then floor -- the same
 // doubles as the reference's, bit for bit, from the frame's binary64 bits.
@@ -789,19 +755,19 @@ void launch_trav_tree(cudaStream_t s, const DevState &S, ScanScratch &scan, bool
 void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
                   SortScratch &sort, bool moments) {
   const uint32_t n = S.n;
-  launch_bounds(s, S);
-  k_root_frame<<<(S.nseg + 127) / 128, 128, 0, s>>>(S);
+  launch_bounds(s, S); // and the root frames (its last block)
   mark(s, "build.bounds");
-  cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * 4 * 256, s);
+  // digit rows, tile counters, look-back words and the long-run count were
+  // cleared by the step prologue (launch_step_zero)
   k_morton<<<grid_for(n), kBlock, 0, s>>>(S, keys32(sort, 0), sort.hist);
   mark(s, "build.morton");
   // radix passes over the codes' high 32 bits (depth-16 cells), then every
   // run of equal high bits is ordered by its low bits: the same stable order
   // as a full 64-bit sort; such runs are rare and short (at most 2 bodies in
   // the headline states), so this replaces four full passes
-  int buf = radix_sort_u32(s, sort, n, nullptr, 0, 32, true, true, S.status);
+  int buf = radix_sort_u32(s, sort, n, nullptr, 0, 32, true, true, S.status, 0, true);
   sort_fix_low_bits32(s, sort, buf, n, S.codes, S.longRuns, &S.counters[9], n / 16 + 64,
-                      S.status);
+                      S.status, true);
   mark(s, "build.sort");
   if (S.nseg > 1) {
     // stable passes on the instance id keep instances in their ranges

@@ -664,7 +664,8 @@ __global__ void __launch_bounds__(kBlock)
 
 // Bounding boxes per instance: each block takes a contiguous chunk;
 // per-thread min/max keys, block-reduced when the whole block is in one
-// instance, flushed with atomics otherwise.
+// instance, flushed with atomics otherwise.  The last block to finish sets
+// every instance's root square and Morton frame (root_frame_seg).
 __global__ void __launch_bounds__(kBlock) k_bounds(DevState S) {
   const uint32_t n = S.n;
   const uint32_t chunk = (n + gridDim.x - 1) / gridDim.x;
@@ -728,13 +729,25 @@ __global__ void __launch_bounds__(kBlock) k_bounds(DevState S) {
     }
   }
   __syncthreads();
-  if (threadIdx.x == 0 && sSeg != 0xffffffffu && sb[1] != 0u) {
-    uint32_t *b = S.bounds + 4 * sSeg;
-    atomicMin(b + 0, sb[0]);
-    atomicMax(b + 1, sb[1]);
-    atomicMin(b + 2, sb[2]);
-    atomicMax(b + 3, sb[3]);
+  __shared__ bool sLast;
+  if (threadIdx.x == 0) {
+    if (sSeg != 0xffffffffu && sb[1] != 0u) {
+      uint32_t *b = S.bounds + 4 * sSeg;
+      atomicMin(b + 0, sb[0]);
+      atomicMax(b + 1, sb[1]);
+      atomicMin(b + 2, sb[2]);
+      atomicMax(b + 3, sb[3]);
+    }
+    // this block's bounds before its arrival; the last block to arrive
+    // sees every block's bounds
+    __threadfence();
+    sLast = atomicAdd(&S.counters[kCtrBoundsDone], 1u) == gridDim.x - 1;
   }
+  __syncthreads();
+  if (!sLast) return;
+  __threadfence();
+  for (uint32_t sg = threadIdx.x; sg < S.nseg; sg += blockDim.x) root_frame_seg(S, sg);
+  if (threadIdx.x == 0) S.counters[kCtrBoundsDone] = 0u;
 }
 
 int grid_for(uint32_t n) {
@@ -743,9 +756,59 @@ int grid_for(uint32_t n) {
   return b ? (int)b : 1;
 }
 
+struct ZeroRanges {
+  uint32_t *p[8];
+  uint32_t n[8];
+  int count;
+};
+
+// Clears every range (16-byte aligned ranges with 16-byte stores).
+__global__ void __launch_bounds__(kBlock) k_zero_ranges(ZeroRanges z) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (int r = 0; r < z.count; ++r) {
+    uint32_t *p = z.p[r];
+    const uint32_t n = z.n[r];
+    uint32_t head = 0;
+    if ((reinterpret_cast<uintptr_t>(p) & 15u) == 0) {
+      uint4 *q = reinterpret_cast<uint4 *>(p);
+      for (uint32_t i = t; i < n / 4; i += stride) q[i] = make_uint4(0u, 0u, 0u, 0u);
+      head = n & ~3u;
+    }
+    for (uint32_t i = head + t; i < n; i += stride) p[i] = 0u;
+  }
+}
+
 } // namespace
 
 // Host-side sequencing of the collision phase (no host synchronisation).
+
+// What a step's phases expect cleared, in one launch: the collision
+// counters (units, unit claims, small-large pairs, long runs of both
+// sorts) and both sorts' digit rows, tile counters and look-back words
+// (the Morton sort in slots 0-3, the units' in 4-6); with grid, also the
+// collision grid's bucket and large counts (a step or phase that collides).
+void launch_step_zero(cudaStream_t s, const DevState &S, SortScratch &sort, bool grid) {
+  ZeroRanges z{};
+  auto add = [&](uint32_t *p, size_t n) {
+    z.p[z.count] = p;
+    z.n[z.count] = (uint32_t)n;
+    ++z.count;
+  };
+  if (grid) {
+    add(S.bucketCount, S.nBuckets + 1);
+    add(S.largeCount, S.nseg);
+  }
+  add(S.counters + 1, 2); // units, unit claims
+  add(S.counters + 5, 1); // small-large pairs
+  add(S.counters + 9, 2); // long runs of the Morton and the units' sorts
+  add(sort.hist, 7 * 256);
+  add(sort.tileCounter, 8);
+  const uint32_t statusWords = 7 * (uint32_t)sort_pass_words(S.n);
+  add(sort.status, statusWords);
+  const uint32_t big = grid && S.nBuckets + 1 > statusWords ? S.nBuckets + 1 : statusWords;
+  k_zero_ranges<<<grid_for(big / 4 + 1), kBlock, 0, s>>>(z);
+}
+
 void launch_integrate(cudaStream_t s, const DevState &S, bool integrate,
                       bool collide) {
   k_integrate_boxes<<<grid_for(S.n), kBlock, 0, s>>>(S, integrate ? 1 : 0,
@@ -763,28 +826,26 @@ void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
   k_fill_grid<<<grid_for(n), kBlock, 0, s>>>(S);
   mark(s, "collide.grid");
   // partners: count (+ stash), scan, fill + sort
-  cudaMemsetAsync(&S.counters[5], 0, sizeof(uint32_t), s);
   k_partners_count<<<grid_for(n), kBlock, 0, s>>>(S);
   exclusive_scan_u32(s, S.deg, S.pstart, n, nullptr, &S.counters[0], scan,
                      S.status);
   mark(s, "collide.count");
   // the fill kernels also write every body's key for the units' sort
   // (units first, in before() order) and its digit histograms
-  cudaMemsetAsync(sort.hist, 0, sizeof(uint32_t) * 3 * 256, s);
-  cudaMemsetAsync(&S.counters[1], 0, sizeof(uint32_t), s);
-  k_partners_fill<<<grid_for(n), kBlock, 0, s>>>(S, keys32(sort, 0), sort.hist);
+  uint32_t *unitHist = sort.hist + kUnitSortSlot * 256;
+  k_partners_fill<<<grid_for(n), kBlock, 0, s>>>(S, keys32(sort, 0), unitHist);
   k_fill_large_pairs<<<64, kBlock, 0, s>>>(S);
-  k_sort_large<<<64, kBlock, 0, s>>>(S, keys32(sort, 0), sort.hist);
+  k_sort_large<<<64, kBlock, 0, s>>>(S, keys32(sort, 0), unitHist);
   mark(s, "collide.fill");
   // units in before() order: a stable sort of all bodies' coarse keys
   // (value = index), then each run of equal coarse keys in exact minX order;
   // the first counters[1] entries are the units
-  const int buf = radix_sort_u32(s, sort, n, nullptr, 0, 24, true, true, S.status);
-  sort_fix_units(s, sort, buf, n, S.box, kNonUnitKey, S.longRuns, &S.counters[9],
-                 n / 16 + 64, S.status);
+  const int buf = radix_sort_u32(s, sort, n, nullptr, 0, 24, true, true, S.status,
+                                 kUnitSortSlot, true);
+  sort_fix_units(s, sort, buf, n, S.box, kNonUnitKey, S.longRuns, &S.counters[10],
+                 n / 16 + 64, S.status, true);
   mark(s, "collide.units");
   // ordered resolution
-  cudaMemsetAsync(&S.counters[2], 0, sizeof(uint32_t), s);
   k_twins<<<grid_for(n), kBlock, 0, s>>>(S);
   k_resolve<<<148 * 8, kBlock, 0, s>>>(S, sort.vals[buf]);
   mark(s, "collide.resolve");

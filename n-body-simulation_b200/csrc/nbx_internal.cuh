@@ -130,16 +130,25 @@ struct SortScratch {
 };
 
 size_t sort_tiles(uint32_t n_max);
+// Look-back words of one pass over n_max keys (one slot of scratch.status).
+size_t sort_pass_words(uint32_t n_max);
+// Scratch slots of a step's two sorts: the Morton codes' passes use slots
+// 0-3, the contact units' slots 4-6 (cleared together by the step prologue).
+constexpr int kUnitSortSlot = 4;
 
 // Stable LSD radix sort of (keys[0], vals[0]) on key bits [bit_lo, bit_hi)
-// (multiples of 8).  If `have_hist` the caller already filled
-// scratch.hist for those passes (e.g. fused into the key-producing
-// kernel) and zeroed nothing else.  vals_identity: vals[0] is not read,
-// value = original index.  Returns the buffer index (0/1) holding the
-// result.
+// (multiples of 8).  If `have_hist` the caller already filled the digit
+// counts for those passes (e.g. fused into the key-producing kernel).
+// vals_identity: vals[0] is not read, value = original index.  The passes
+// use the scratch's digit rows, look-back slots and tile counters from
+// `slot` on (pass p of the key: row slot + bit_lo / 8 + p, slot and counter
+// slot + p); with `zeroed` the caller has cleared those (the step
+// prologue), else the sort does.  Returns the buffer index (0/1) holding
+// the result.
 int radix_sort_u64(cudaStream_t s, SortScratch &sc, uint32_t n_max,
                    const uint32_t *d_n, int bit_lo, int bit_hi,
-                   bool vals_identity, bool have_hist, uint32_t *err);
+                   bool vals_identity, bool have_hist, uint32_t *err,
+                   int slot = 0, bool zeroed = false);
 
 // The same sort with 32-bit keys, held in the key buffers' storage
 // (keys32): two thirds of the bytes per pass of 64-bit keys.
@@ -148,7 +157,8 @@ inline uint32_t *keys32(SortScratch &sc, int buf) {
 }
 int radix_sort_u32(cudaStream_t s, SortScratch &sc, uint32_t n_max,
                    const uint32_t *d_n, int bit_lo, int bit_hi,
-                   bool vals_identity, bool have_hist, uint32_t *err);
+                   bool vals_identity, bool have_hist, uint32_t *err,
+                   int slot = 0, bool zeroed = false);
 
 // Completes a stable sort of 64-bit codes that ran its radix passes on the
 // high 32 bits only (keys32(sc, buf) = codes[vals] >> 32, sorted): every run
@@ -156,7 +166,7 @@ int radix_sort_u32(cudaStream_t s, SortScratch &sc, uint32_t n_max,
 // in place.  longRuns holds cap run starts; *runCount is device scratch.
 void sort_fix_low_bits32(cudaStream_t s, SortScratch &sc, int buf, uint32_t n,
                          const uint64_t *codes, uint32_t *longRuns, uint32_t *runCount,
-                         uint32_t cap, uint32_t *err);
+                         uint32_t cap, uint32_t *err, bool zeroed = false);
 
 // The same for the contact units, whose radix passes ran on a coarse,
 // order-preserving key of the box's minX: every run of equal coarse keys
@@ -164,6 +174,6 @@ void sort_fix_low_bits32(cudaStream_t s, SortScratch &sc, int buf, uint32_t n,
 // order key, stably (ties keep index order).
 void sort_fix_units(cudaStream_t s, SortScratch &sc, int buf, uint32_t n, const float4 *box,
                     uint32_t skip, uint32_t *longRuns, uint32_t *runCount, uint32_t cap,
-                    uint32_t *err);
+                    uint32_t *err, bool zeroed = false);
 
 } // namespace nbx

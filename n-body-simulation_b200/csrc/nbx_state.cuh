@@ -3,6 +3,8 @@
 #pragma once
 #include "nbx_internal.cuh"
 
+#include <float.h>
+
 namespace nbx {
 
 // Per-segment record in device memory.
@@ -48,6 +50,7 @@ constexpr int kLevelSlots = 34; // depths 0..32 plus an end slot
 // (float bits), and each build marks the instances whose bodies reach
 // beyond it (SegDev::wide), for the force pass to keep the clamp there.
 constexpr int kCtrCoordLimit = 15;
+constexpr int kCtrBoundsDone = 7; // blocks of the bounds pass done (self-resetting)
 
 // Everything a step's kernels touch.  All pointers are device pointers.
 struct DevState {
@@ -113,6 +116,7 @@ struct DevState {
                          // [5]=small-large pairs [6]=traversal records
                          // [8]=id check
                          // [9]=long Morton runs [12]=upload mass bits
+                         // [7]=bounds blocks done [10]=long unit runs
                          // [13]=expiry test flag [kCtrCoordLimit] (above)
 
   // Morton / sort
@@ -177,6 +181,39 @@ __device__ __forceinline__ void add_attractor(const float4 *attr, float px, floa
     ax = fmaf(dx, f, ax);
     ay = fmaf(dy, f, ay);
   }
+}
+
+__device__ __forceinline__ float key_to_float(uint32_t k) {
+  return u2f((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// Root square of instance sg (Quad::newContaining, QuadTree.cpp:30-51, and
+// rootSquare, CudaQuadTree.cu:25-30) and its Morton frame, from the step's
+// bound accumulators, which it resets for the next step.
+__device__ __forceinline__ void root_frame_seg(const DevState &S, uint32_t sg) {
+  uint32_t *b = S.bounds + 4 * sg;
+  const uint32_t k0 = __ldcg(b), k1 = __ldcg(b + 1), k2 = __ldcg(b + 2), k3 = __ldcg(b + 3);
+  const float minX = k0 == 0xffffffffu ? FLT_MAX : key_to_float(k0);
+  const float maxX = k1 == 0u ? -FLT_MAX : key_to_float(k1);
+  const float minY = k2 == 0xffffffffu ? FLT_MAX : key_to_float(k2);
+  const float maxY = k3 == 0u ? -FLT_MAX : key_to_float(k3);
+  const float cx = __fmul_rn(__fadd_rn(minX, maxX), 0.5f);
+  const float cy = __fmul_rn(__fadd_rn(minY, maxY), 0.5f);
+  const float w = __fsub_rn(maxX, minX), h = __fsub_rn(maxY, minY);
+  const float size = (w < h) ? h : w;
+  SegDev &G = S.seg[sg];
+  G.cx = cx;
+  G.cy = cy;
+  G.size = size;
+  G.frame = sd_morton_frame(cx, cy, size);
+  // clamp guard: bodies beyond the upload's coordinate limit (NaN-safe)
+  const float lim = __uint_as_float(S.counters[kCtrCoordLimit]);
+  const float reach = fmaxf(fmaxf(fabsf(minX), fabsf(maxX)), fmaxf(fabsf(minY), fabsf(maxY)));
+  G.wide = (k0 != 0xffffffffu && !(reach < lim)) ? 1u : 0u;
+  b[0] = 0xffffffffu;
+  b[1] = 0u;
+  b[2] = 0xffffffffu;
+  b[3] = 0u;
 }
 
 } // namespace nbx

@@ -172,22 +172,6 @@ __global__ void k_radix_hist(const K *__restrict__ keys, uint32_t n_max,
   }
 }
 
-// hist[p][*] -> exclusive digit starts, in place.
-__global__ void k_radix_hist_scan(uint32_t *hist, int pass_lo) {
-  __shared__ uint32_t s[256];
-  uint32_t *h = hist + (pass_lo + blockIdx.x) * 256;
-  const int t = threadIdx.x;
-  s[t] = h[t];
-  __syncthreads();
-  for (int o = 1; o < 256; o <<= 1) {
-    const uint32_t v = t >= o ? s[t - o] : 0u;
-    __syncthreads();
-    s[t] += v;
-    __syncthreads();
-  }
-  h[t] = s[t] - h[t];
-}
-
 // At least 3 blocks per SM (<= 85 registers): a 1M-key pass (342 tiles)
 // is then resident in one wave on 148 SMs.
 template <typename K, bool kIdentity>
@@ -195,7 +179,7 @@ __global__ void __launch_bounds__(kSortThreads, 3)
     k_onesweep(const K *__restrict__ keysIn,
                const uint32_t *__restrict__ valsIn,
                K *__restrict__ keysOut, uint32_t *__restrict__ valsOut,
-               const uint32_t *__restrict__ digitStart, uint32_t *status,
+               const uint32_t *__restrict__ digitCount, uint32_t *status,
                uint32_t *tileCounter, uint32_t n_max, const uint32_t *d_n,
                int shift, uint32_t *err) {
   __shared__ K s_keys[kSortTile];
@@ -213,6 +197,8 @@ __global__ void __launch_bounds__(kSortThreads, 3)
   __syncthreads();
   const uint32_t tile = s_tile;
   if (tile >= numTiles) return;
+  // the pass's count of digit tid over the whole array (kSortThreads == 256)
+  const uint32_t digitTotal = digitCount[tid];
   const uint32_t base = tile * kSortTile;
   const uint32_t wbase = base + warp * (kSortItems * 32);
 
@@ -271,20 +257,33 @@ __global__ void __launch_bounds__(kSortThreads, 3)
     st_relaxed_u32(status + (size_t)tile * 256 + d,
                    ((tile == 0 ? 2u : 1u) << kRFlagShift) | count);
   }
-  // exclusive scan of tile counts over digits (256 entries, one per thread)
+  // exclusive scans over digits (256 entries, one per thread) of the tile's
+  // counts and of the pass's whole-array counts (the digit's global start)
+  uint32_t digitStart;
   {
-    uint32_t inc = count;
+    uint32_t inc = count, incAll = digitTotal;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
-      if (lane >= o) inc += t;
+      const uint32_t tAll = __shfl_up_sync(0xffffffffu, incAll, o);
+      if (lane >= o) {
+        inc += t;
+        incAll += tAll;
+      }
     }
-    __shared__ uint32_t s_wsum[kSortWarps];
-    if (lane == 31) s_wsum[warp] = inc;
+    __shared__ uint32_t s_wsum[kSortWarps], s_wsumAll[kSortWarps];
+    if (lane == 31) {
+      s_wsum[warp] = inc;
+      s_wsumAll[warp] = incAll;
+    }
     __syncthreads();
-    uint32_t off = 0;
-    for (int w = 0; w < warp; ++w) off += s_wsum[w];
+    uint32_t off = 0, offAll = 0;
+    for (int w = 0; w < warp; ++w) {
+      off += s_wsum[w];
+      offAll += s_wsumAll[w];
+    }
     s_local[tid] = off + inc - count;
+    digitStart = offAll + incAll - digitTotal;
   }
   __syncthreads();
   // local reorder by digit (stable)
@@ -337,7 +336,7 @@ __global__ void __launch_bounds__(kSortThreads, 3)
       st_relaxed_u32(status + (size_t)tile * 256 + d,
                      (2u << kRFlagShift) | ((excl + count) & kRValueMask));
     }
-    s_global[d] = digitStart[d] + excl;
+    s_global[d] = digitStart + excl;
   }
   __syncthreads();
   const uint32_t valid = min((uint32_t)kSortTile, n - base);
@@ -506,9 +505,9 @@ __global__ void __launch_bounds__(256)
 
 void sort_fix_low_bits32(cudaStream_t s, SortScratch &sc, int buf, uint32_t n,
                          const uint64_t *codes, uint32_t *longRuns, uint32_t *runCount,
-                         uint32_t cap, uint32_t *err) {
+                         uint32_t cap, uint32_t *err, bool zeroed) {
   if (n < 2) return;
-  cudaMemsetAsync(runCount, 0, sizeof(uint32_t), s);
+  if (!zeroed) cudaMemsetAsync(runCount, 0, sizeof(uint32_t), s);
   uint32_t b = (n + 255) / 256;
   if (b > 148u * 16u) b = 148u * 16u;
   const CodeLow lk{codes};
@@ -520,9 +519,9 @@ void sort_fix_low_bits32(cudaStream_t s, SortScratch &sc, int buf, uint32_t n,
 
 void sort_fix_units(cudaStream_t s, SortScratch &sc, int buf, uint32_t n, const float4 *box,
                     uint32_t skip, uint32_t *longRuns, uint32_t *runCount, uint32_t cap,
-                    uint32_t *err) {
+                    uint32_t *err, bool zeroed) {
   if (n < 2) return;
-  cudaMemsetAsync(runCount, 0, sizeof(uint32_t), s);
+  if (!zeroed) cudaMemsetAsync(runCount, 0, sizeof(uint32_t), s);
   uint32_t b = (n + 255) / 256;
   if (b > 148u * 16u) b = 148u * 16u;
   const BoxMinX lk{box};
@@ -536,39 +535,43 @@ size_t sort_tiles(uint32_t n_max) {
   return (n_max + kSortTile - 1) / kSortTile + 1;
 }
 
+size_t sort_pass_words(uint32_t n_max) {
+  return 256 * (size_t)((n_max + kSortTile - 1) / kSortTile + 1);
+}
+
 namespace {
 template <typename K>
 int radix_sort(cudaStream_t s, SortScratch &sc, K *const keys[2], uint32_t n_max,
                const uint32_t *d_n, int bit_lo, int bit_hi, bool vals_identity,
-               bool have_hist, uint32_t *err) {
+               bool have_hist, uint32_t *err, int slot, bool zeroed) {
   const int p0 = bit_lo / 8, np = (bit_hi - bit_lo) / 8;
+  uint32_t *hist = sc.hist + (size_t)(slot + p0) * 256;
   if (!have_hist) {
-    cudaMemsetAsync(sc.hist + p0 * 256, 0, sizeof(uint32_t) * 256 * np, s);
+    if (!zeroed) cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 256 * np, s);
     int blocks = (int)((n_max + 1023) / 1024);
     if (blocks > 1184) blocks = 1184;
     if (blocks < 1) blocks = 1;
-    k_radix_hist<K><<<blocks, 256, 0, s>>>(keys[0], n_max, d_n, p0, np, sc.hist);
+    k_radix_hist<K><<<blocks, 256, 0, s>>>(keys[0], n_max, d_n, p0, np, sc.hist + slot * 256);
   }
-  k_radix_hist_scan<<<np, 256, 0, s>>>(sc.hist, p0);
   const uint32_t tiles = (n_max + kSortTile - 1) / kSortTile;
-  cudaMemsetAsync(sc.tileCounter, 0, sizeof(uint32_t) * 8, s);
   // look-back words of every pass, cleared at once
-  const size_t passWords = 256 * (size_t)(tiles + 1);
-  cudaMemsetAsync(sc.status, 0, sizeof(uint32_t) * passWords * np, s);
+  const size_t passWords = sort_pass_words(n_max);
+  if (!zeroed) {
+    cudaMemsetAsync(sc.tileCounter + slot, 0, sizeof(uint32_t) * np, s);
+    cudaMemsetAsync(sc.status + passWords * slot, 0, sizeof(uint32_t) * passWords * np, s);
+  }
   int cur = 0;
   for (int p = 0; p < np; ++p) {
-    uint32_t *status = sc.status + passWords * p;
+    uint32_t *status = sc.status + passWords * (slot + p);
     const int shift = 8 * (p0 + p);
     if (p == 0 && vals_identity) {
       k_onesweep<K, true><<<tiles > 0 ? tiles : 1, kSortThreads, 0, s>>>(
-          keys[cur], sc.vals[cur], keys[cur ^ 1], sc.vals[cur ^ 1],
-          sc.hist + (p0 + p) * 256, status, sc.tileCounter + p, n_max, d_n,
-          shift, err);
+          keys[cur], sc.vals[cur], keys[cur ^ 1], sc.vals[cur ^ 1], hist + p * 256, status,
+          sc.tileCounter + slot + p, n_max, d_n, shift, err);
     } else {
       k_onesweep<K, false><<<tiles > 0 ? tiles : 1, kSortThreads, 0, s>>>(
-          keys[cur], sc.vals[cur], keys[cur ^ 1], sc.vals[cur ^ 1],
-          sc.hist + (p0 + p) * 256, status, sc.tileCounter + p, n_max, d_n,
-          shift, err);
+          keys[cur], sc.vals[cur], keys[cur ^ 1], sc.vals[cur ^ 1], hist + p * 256, status,
+          sc.tileCounter + slot + p, n_max, d_n, shift, err);
     }
     cur ^= 1;
   }
@@ -578,17 +581,17 @@ int radix_sort(cudaStream_t s, SortScratch &sc, K *const keys[2], uint32_t n_max
 
 int radix_sort_u64(cudaStream_t s, SortScratch &sc, uint32_t n_max,
                    const uint32_t *d_n, int bit_lo, int bit_hi,
-                   bool vals_identity, bool have_hist, uint32_t *err) {
+                   bool vals_identity, bool have_hist, uint32_t *err, int slot, bool zeroed) {
   return radix_sort<uint64_t>(s, sc, sc.keys, n_max, d_n, bit_lo, bit_hi, vals_identity,
-                              have_hist, err);
+                              have_hist, err, slot, zeroed);
 }
 
 int radix_sort_u32(cudaStream_t s, SortScratch &sc, uint32_t n_max,
                    const uint32_t *d_n, int bit_lo, int bit_hi,
-                   bool vals_identity, bool have_hist, uint32_t *err) {
+                   bool vals_identity, bool have_hist, uint32_t *err, int slot, bool zeroed) {
   uint32_t *const keys[2] = {keys32(sc, 0), keys32(sc, 1)};
   return radix_sort<uint32_t>(s, sc, keys, n_max, d_n, bit_lo, bit_hi, vals_identity,
-                              have_hist, err);
+                              have_hist, err, slot, zeroed);
 }
 
 } // namespace nbx
