@@ -29,7 +29,8 @@ void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
                   SortScratch &sort, bool moments);
 void launch_bfs_tree(cudaStream_t s, const DevState &S, ScanScratch &scan,
                      SortScratch &sort);
-void launch_step_zero(cudaStream_t s, const DevState &S, SortScratch &sort, bool grid);
+void launch_step_zero(cudaStream_t s, const DevState &S, ScanScratch &scan, SortScratch &sort,
+                      bool grid);
 void launch_forces(cudaStream_t s, const DevState &S, bool exact, int blocks,
                    const MlpDev *mlp, float band, int corr, bool noClamp, int threads,
                    bool pairs);
@@ -434,6 +435,8 @@ int allocate(nbx_handle *h) {
   ScanScratch &sc = h->scan;
   sc.maxTiles = (uint32_t)scan_scratch_tiles(std::max<uint32_t>(S.nBuckets + 2, sortCap));
   A(sc.status, sc.maxTiles + 1);
+  A(sc.slotStatus, (size_t)kScanSlots * sc.maxTiles);
+  A(sc.tileCounter, kScanSlots);
   A(sc.tileCounter, 1);
   A(h->dAoS, n);
   A(h->dF64, 16 * 592);
@@ -540,7 +543,7 @@ void enqueue_forces_io(nbx_handle *h, cudaStream_t s, const DevState &S) {
 // One Simulation::step on stream s for state S; returns the state after the
 // Morton gather's buffer swap.
 DevState enqueue_step(nbx_handle *h, cudaStream_t s, DevState S) {
-  launch_step_zero(s, S, h->sort, S.collisions != 0);
+  launch_step_zero(s, S, h->scan, h->sort, S.collisions != 0);
   launch_integrate(s, S, true, S.collisions != 0);
   mark(s, "integrate");
   if (S.collisions) launch_collide(s, S, h->scan, h->sort);
@@ -1429,7 +1432,7 @@ int nbx_phase(nbx_handle *h, int phase) {
     launch_integrate(s, S, true, false);
     break;
   case NBX_PHASE_COLLIDE:
-    launch_step_zero(s, S, h->sort, true);
+    launch_step_zero(s, S, h->scan, h->sort, true);
     launch_integrate(s, S, false, true);
     launch_collide(s, S, h->scan, h->sort);
     h->collideValid = true;
@@ -1442,7 +1445,7 @@ int nbx_phase(nbx_handle *h, int phase) {
       h->forceInput = true;
       break;
     }
-    launch_step_zero(s, S, h->sort, false);
+    launch_step_zero(s, S, h->scan, h->sort, false);
     launch_build(s, S, h->scan, h->sort, true);
     h->momentsValid = true;
     h->cur ^= 1;
@@ -1471,7 +1474,7 @@ int nbx_phase(nbx_handle *h, int phase) {
       launch_naive_forces(s, S, h->params.exact_math != 0);
       break;
     }
-    launch_step_zero(s, S, h->sort, false);
+    launch_step_zero(s, S, h->scan, h->sort, false);
     launch_build(s, S, h->scan, h->sort, true);
     h->momentsValid = true;
     h->cur ^= 1;

@@ -806,7 +806,7 @@ void launch_trav_tree(cudaStream_t s, const DevState &S, ScanScratch &scan, bool
   k_trav_counts<<<grid_for(n), kBlock, 0, s>>>(S);
   // the scan also writes each record's first body (owner)
   exclusive_scan_u32(s, S.splitCount, S.splitStart, n, nullptr, &S.counters[6],
-                     scan, S.status, owner, S.nodeCapacity);
+                     scan, S.status, owner, S.nodeCapacity, 3);
   mark(s, "tree.counts");
   if (moments)
     k_trav_nodes<true><<<grid_for(n / 2 + 64), kBlock, 0, s>>>(S, owner, kids);

@@ -268,9 +268,6 @@ __global__ void __launch_bounds__(kBlock) k_partners_count(DevState S) {
   }
 }
 
-// Fill pass: small bodies copy their stash (or search again past kStash
-// partners) into their CSR list and sort it by the partners' before()
-// order; large bodies add their large-large partners.
 // Coarse sort key of a unit's minX: 24 bits over twice the instance's last
 // root square, order-preserving (a float subtract, a multiply by a positive
 // scale and floor are each monotone), clamped at the ends.  The sort on it
@@ -312,6 +309,11 @@ __device__ __forceinline__ void flush_unit_hist(uint32_t (*sh)[256], uint32_t un
   if (threadIdx.x == 0 && *sUnits) atomicAdd(unitCount, *sUnits);
 }
 
+// Fill pass: small bodies copy their stash (or search again past kStash
+// partners) into their CSR list and sort it by the partners' before()
+// order; large bodies add their large-large partners, and the count pass's
+// small-large pairs go into the large bodies' lists.  Every body's unit
+// key and its digit counts come out too.
 __global__ void __launch_bounds__(kBlock)
     k_partners_fill(DevState S, uint32_t *__restrict__ keys, uint32_t *hist) {
   __shared__ uint32_t sh[3][256];
@@ -382,19 +384,18 @@ __global__ void __launch_bounds__(kBlock)
     S.nLater[i] = nl;
     unit_key(i, nl > 0, S.seg[sg], bi.x, keys, sh, units);
   }
-  flush_unit_hist(sh, units, &sUnits, hist, &S.counters[1]);
-}
-
-// Small-large pairs recorded by the count pass, into the large lists.
-__global__ void __launch_bounds__(kBlock) k_fill_large_pairs(DevState S) {
-  if (S.counters[0] > S.pairCapacity) return;
-  const uint32_t total = min(S.counters[5], S.n);
-  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total;
-       p += gridDim.x * blockDim.x) {
-    const uint2 pr = S.largePairs[p];
-    const uint32_t slot = atomicAdd(&S.fillLarge[pr.x], 1u);
-    S.plist[S.pstart[pr.x] + slot] = pr.y;
+  // the small-large pairs recorded by the count pass, into the large
+  // bodies' lists (in any order: k_sort_large orders those lists)
+  if (!overflow) {
+    const uint32_t total = min(S.counters[5], S.n);
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += gridDim.x * blockDim.x) {
+      const uint2 pr = S.largePairs[q];
+      const uint32_t slot = atomicAdd(&S.fillLarge[pr.x], 1u);
+      S.plist[S.pstart[pr.x] + slot] = pr.y;
+    }
   }
+  flush_unit_hist(sh, units, &sUnits, hist, &S.counters[1]);
 }
 
 // Sorts each large body's partner list (filled by others through atomics)
@@ -757,8 +758,8 @@ int grid_for(uint32_t n) {
 }
 
 struct ZeroRanges {
-  uint32_t *p[8];
-  uint32_t n[8];
+  uint32_t *p[12];
+  uint32_t n[12];
   int count;
 };
 
@@ -784,10 +785,13 @@ __global__ void __launch_bounds__(kBlock) k_zero_ranges(ZeroRanges z) {
 
 // What a step's phases expect cleared, in one launch: the collision
 // counters (units, unit claims, small-large pairs, long runs of both
-// sorts) and both sorts' digit rows, tile counters and look-back words
-// (the Morton sort in slots 0-3, the units' in 4-6); with grid, also the
-// collision grid's bucket and large counts (a step or phase that collides).
-void launch_step_zero(cudaStream_t s, const DevState &S, SortScratch &sort, bool grid) {
+// sorts), both sorts' digit rows, tile counters and look-back words (the
+// Morton sort in slots 0-3, the units' in 4-6) and the four scan slots
+// (grid buckets, large lists, partner lists, traversal records); with
+// grid, also the collision grid's bucket and large counts (a step or phase
+// that collides).
+void launch_step_zero(cudaStream_t s, const DevState &S, ScanScratch &scan, SortScratch &sort,
+                      bool grid) {
   ZeroRanges z{};
   auto add = [&](uint32_t *p, size_t n) {
     z.p[z.count] = p;
@@ -805,6 +809,8 @@ void launch_step_zero(cudaStream_t s, const DevState &S, SortScratch &sort, bool
   add(sort.tileCounter, 8);
   const uint32_t statusWords = 7 * (uint32_t)sort_pass_words(S.n);
   add(sort.status, statusWords);
+  add(reinterpret_cast<uint32_t *>(scan.slotStatus), 2 * (size_t)kScanSlots * scan.maxTiles);
+  add(scan.tileCounter, kScanSlots);
   const uint32_t big = grid && S.nBuckets + 1 > statusWords ? S.nBuckets + 1 : statusWords;
   k_zero_ranges<<<grid_for(big / 4 + 1), kBlock, 0, s>>>(z);
 }
@@ -820,21 +826,20 @@ void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
   const uint32_t n = S.n;
   // grid buckets and large lists
   exclusive_scan_u32(s, S.bucketCount, S.bucketStart, S.nBuckets + 1, nullptr,
-                     nullptr, scan, S.status);
+                     nullptr, scan, S.status, nullptr, 0, 0);
   exclusive_scan_u32(s, S.largeCount, S.largeStartA, S.nseg, nullptr, nullptr,
-                     scan, S.status);
+                     scan, S.status, nullptr, 0, 1);
   k_fill_grid<<<grid_for(n), kBlock, 0, s>>>(S);
   mark(s, "collide.grid");
   // partners: count (+ stash), scan, fill + sort
   k_partners_count<<<grid_for(n), kBlock, 0, s>>>(S);
   exclusive_scan_u32(s, S.deg, S.pstart, n, nullptr, &S.counters[0], scan,
-                     S.status);
+                     S.status, nullptr, 0, 2);
   mark(s, "collide.count");
   // the fill kernels also write every body's key for the units' sort
   // (units first, in before() order) and its digit histograms
   uint32_t *unitHist = sort.hist + kUnitSortSlot * 256;
   k_partners_fill<<<grid_for(n), kBlock, 0, s>>>(S, keys32(sort, 0), unitHist);
-  k_fill_large_pairs<<<64, kBlock, 0, s>>>(S);
   k_sort_large<<<64, kBlock, 0, s>>>(S, keys32(sort, 0), unitHist);
   mark(s, "collide.fill");
   // units in before() order: a stable sort of all bodies' coarse keys

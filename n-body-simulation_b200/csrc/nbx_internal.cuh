@@ -96,9 +96,13 @@ __device__ __forceinline__ uint32_t load_count(const uint32_t *d_n, uint32_t n) 
 // synchronise with the host, so they can be captured in a CUDA graph.
 struct ScanScratch {
   uint64_t *status = nullptr; // per tile: its sum (low 32 bits used)
-  uint32_t *tileCounter = nullptr;
+  uint32_t *tileCounter = nullptr; // [kScanSlots] tile claims of the slots
+  uint64_t *slotStatus = nullptr;  // [kScanSlots][maxTiles] look-back words
   uint32_t maxTiles = 0;
 };
+// Scans with a slot of their own (a step's four scans): one launch each,
+// over look-back words and a tile counter that the step prologue clears.
+constexpr int kScanSlots = 4;
 
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;
@@ -108,10 +112,14 @@ constexpr int kScanTile = kScanThreads * kScanItems;
 // n is *d_n when d_n != nullptr (n_max bounds the launch).  With owner,
 // owner[out[i] + k] = i for k < in[i] (below owner_cap): the element that
 // each unit of the scanned counts belongs to.
+// With slot >= 0 the scan is one launch (decoupled look-back over that
+// slot's words, which must be clear: the step prologue clears all slots);
+// otherwise two (tile sums, then every tile's prefix), needing nothing
+// cleared.
 void exclusive_scan_u32(cudaStream_t s, const uint32_t *in, uint32_t *out,
                         uint32_t n_max, const uint32_t *d_n, uint32_t *total,
                         ScanScratch &sc, uint32_t *err, uint32_t *owner = nullptr,
-                        uint32_t owner_cap = 0);
+                        uint32_t owner_cap = 0, int slot = -1);
 size_t scan_scratch_tiles(uint32_t n_max);
 
 constexpr int kSortThreads = 256;

@@ -2,6 +2,8 @@
 //
 // The scan reduces every tile first and then lets each tile add the sums
 // of the tiles before it: two launches with no dependence between tiles.
+// A step's own scans, whose look-back words the step prologue clears, run
+// as one launch with decoupled look-back instead.
 // The radix sort uses decoupled look-back (Merrill & Garland 2016; Adinets &
 // Merrill 2022, "Onesweep"): tiles are claimed in order through an atomic
 // counter, each tile publishes its digit counts, and looks back over its
@@ -124,6 +126,115 @@ __global__ void __launch_bounds__(kScanThreads)
   }
 }
 
+// One-launch scan: tiles are claimed in launch order through the slot's
+// counter; each publishes its sum at once, and warp 0 looks back over its
+// predecessors' words (32 per round trip) until it meets an inclusive sum,
+// then publishes its own inclusive sum.  Every wait is bounded.
+constexpr uint64_t kScanAggregate = 1ull << 32, kScanInclusive = 2ull << 32;
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan_onepass(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
+                   uint32_t n_max, const uint32_t *d_n, uint32_t *total, uint64_t *status,
+                   uint32_t *tileCounter, uint32_t *__restrict__ owner, uint32_t ownerCap,
+                   uint32_t *err) {
+  __shared__ uint32_t s_items[kScanTile];
+  __shared__ uint32_t s_warp[kScanThreads / 32];
+  __shared__ uint32_t s_tile, s_excl;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = atomicAdd(tileCounter, 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint32_t n = load_count(d_n, n_max);
+  const uint32_t numTiles = (n + kScanTile - 1) / kScanTile;
+  if (n == 0) {
+    if (tile == 0 && tid == 0 && total) *total = 0;
+    return;
+  }
+  if (tile >= numTiles) return;
+  const uint32_t base = tile * kScanTile;
+  for (int k = 0; k < kScanItems; ++k) {
+    const uint32_t i = base + k * kScanThreads + tid;
+    s_items[k * kScanThreads + tid] = i < n ? in[i] : 0u;
+  }
+  __syncthreads();
+  uint32_t v[kScanItems];
+  uint32_t sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = s_items[tid * kScanItems + k];
+    sum += v[k];
+  }
+  uint32_t inc = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  uint32_t woff = 0, blockTotal = 0;
+  for (int w = 0; w < kScanThreads / 32; ++w) {
+    if (w < warp) woff += s_warp[w];
+    blockTotal += s_warp[w];
+  }
+  if (warp == 0) {
+    uint32_t excl = 0;
+    if (tile == 0) {
+      if (lane == 0) st_relaxed_u64(status, kScanInclusive | blockTotal);
+    } else {
+      if (lane == 0) st_relaxed_u64(status + tile, kScanAggregate | blockTotal);
+      int pred = (int)tile - 1;
+      uint32_t spins = 0;
+      for (;;) {
+        const int q = pred - lane;
+        const uint64_t w = q >= 0 ? ld_relaxed_u64(status + q) : kScanInclusive;
+        const uint32_t flag = (uint32_t)(w >> 32);
+        const uint32_t ready = __ballot_sync(0xffffffffu, flag != 0u);
+        const uint32_t incl = __ballot_sync(0xffffffffu, flag == 2u);
+        // the lanes up to the nearest inclusive word, which must all be
+        // published; all 32 when none is inclusive yet
+        const uint32_t upto = incl ? (incl & (0u - incl)) * 2u - 1u : 0xffffffffu;
+        if ((ready & upto) == upto) {
+          uint32_t x = (upto >> lane) & 1u ? (uint32_t)w : 0u;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+          excl += x;
+          if (incl) break;
+          pred -= 32;
+        } else if (++spins > kSpinLimit) {
+          if (lane == 0) atomicOr(err, kStatusSpinLimit);
+          break;
+        } else {
+          __nanosleep(32);
+        }
+      }
+      if (lane == 0) st_relaxed_u64(status + tile, kScanInclusive | (uint32_t)(excl + blockTotal));
+    }
+    if (lane == 0) s_excl = excl;
+  }
+  __syncthreads();
+  const uint32_t excl = s_excl;
+  if (total && tile == numTiles - 1 && tid == 0) *total = excl + blockTotal;
+  uint32_t run = excl + woff + (inc - sum);
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    s_items[tid * kScanItems + k] = run;
+    run += v[k];
+  }
+  __syncthreads();
+  for (int k = 0; k < kScanItems; ++k) {
+    const uint32_t i = base + k * kScanThreads + tid;
+    if (i < n) {
+      const uint32_t o = s_items[k * kScanThreads + tid];
+      out[i] = o;
+      if (owner) {
+        const uint32_t c = in[i];
+        for (uint32_t j = 0; j < c && o + j < ownerCap; ++j) owner[o + j] = i;
+      }
+    }
+  }
+}
+
 } // namespace
 
 size_t scan_scratch_tiles(uint32_t n_max) {
@@ -133,10 +244,15 @@ size_t scan_scratch_tiles(uint32_t n_max) {
 void exclusive_scan_u32(cudaStream_t s, const uint32_t *in, uint32_t *out,
                         uint32_t n_max, const uint32_t *d_n, uint32_t *total,
                         ScanScratch &sc, uint32_t *err, uint32_t *owner,
-                        uint32_t owner_cap) {
+                        uint32_t owner_cap, int slot) {
   const uint32_t tiles = (n_max + kScanTile - 1) / kScanTile;
+  if (slot >= 0) {
+    k_scan_onepass<<<tiles > 0 ? tiles : 1, kScanThreads, 0, s>>>(
+        in, out, n_max, d_n, total, sc.slotStatus + (size_t)slot * sc.maxTiles,
+        sc.tileCounter + slot, owner, owner_cap, err);
+    return;
+  }
   uint32_t *tileSum = reinterpret_cast<uint32_t *>(sc.status);
-  (void)err;
   // a single tile adds no earlier tile sums: no reduce pass
   if (tiles > 1)
     k_scan_reduce<<<tiles, kScanThreads, 0, s>>>(in, n_max, d_n, tileSum);
