@@ -25,6 +25,13 @@ namespace nbx {
 namespace {
 
 
+// The tiles' items pass through shared memory between coalesced global
+// accesses (item k * threads + t) and each thread's run of consecutive
+// items (t * items + k); one padding word per 32 keeps both conflict-free
+// (a run's start moves one bank per thread instead of 16).
+constexpr int kScanPadded = kScanTile + kScanTile / 32;
+__device__ __forceinline__ int scan_pad(int i) { return i + (i >> 5); }
+
 // Reduce-then-apply scan: the tile sums first (no dependence between
 // tiles), then every tile adds the sums of the tiles before it (read from
 // L2, summed in shared memory) and scans its items.  Two launches and no
@@ -62,7 +69,7 @@ __global__ void __launch_bounds__(kScanThreads)
                  uint32_t n_max, const uint32_t *d_n, uint32_t *total,
                  const uint32_t *__restrict__ tileSum, uint32_t *__restrict__ owner,
                  uint32_t ownerCap) {
-  __shared__ uint32_t s_items[kScanTile];
+  __shared__ uint32_t s_items[kScanPadded];
   __shared__ uint32_t s_warp[kScanThreads / 32];
   __shared__ uint32_t sh[kScanThreads / 32];
   const int tid = threadIdx.x;
@@ -80,14 +87,14 @@ __global__ void __launch_bounds__(kScanThreads)
   const uint32_t base = tile * kScanTile;
   for (int k = 0; k < kScanItems; ++k) {
     const uint32_t i = base + k * kScanThreads + tid;
-    s_items[k * kScanThreads + tid] = i < n ? in[i] : 0u;
+    s_items[scan_pad(k * kScanThreads + tid)] = i < n ? in[i] : 0u;
   }
   __syncthreads();
   uint32_t v[kScanItems];
   uint32_t sum = 0;
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
-    v[k] = s_items[tid * kScanItems + k];
+    v[k] = s_items[scan_pad(tid * kScanItems + k)];
     sum += v[k];
   }
   const int lane = tid & 31, warp = tid >> 5;
@@ -109,14 +116,14 @@ __global__ void __launch_bounds__(kScanThreads)
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
-    s_items[tid * kScanItems + k] = run;
+    s_items[scan_pad(tid * kScanItems + k)] = run;
     run += v[k];
   }
   __syncthreads();
   for (int k = 0; k < kScanItems; ++k) {
     const uint32_t i = base + k * kScanThreads + tid;
     if (i < n) {
-      const uint32_t o = s_items[k * kScanThreads + tid];
+      const uint32_t o = s_items[scan_pad(k * kScanThreads + tid)];
       out[i] = o;
       if (owner) {
         const uint32_t c = in[i];
@@ -137,7 +144,7 @@ __global__ void __launch_bounds__(kScanThreads)
                    uint32_t n_max, const uint32_t *d_n, uint32_t *total, uint64_t *status,
                    uint32_t *tileCounter, uint32_t *__restrict__ owner, uint32_t ownerCap,
                    uint32_t *err) {
-  __shared__ uint32_t s_items[kScanTile];
+  __shared__ uint32_t s_items[kScanPadded];
   __shared__ uint32_t s_warp[kScanThreads / 32];
   __shared__ uint32_t s_tile, s_excl;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -154,14 +161,14 @@ __global__ void __launch_bounds__(kScanThreads)
   const uint32_t base = tile * kScanTile;
   for (int k = 0; k < kScanItems; ++k) {
     const uint32_t i = base + k * kScanThreads + tid;
-    s_items[k * kScanThreads + tid] = i < n ? in[i] : 0u;
+    s_items[scan_pad(k * kScanThreads + tid)] = i < n ? in[i] : 0u;
   }
   __syncthreads();
   uint32_t v[kScanItems];
   uint32_t sum = 0;
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
-    v[k] = s_items[tid * kScanItems + k];
+    v[k] = s_items[scan_pad(tid * kScanItems + k)];
     sum += v[k];
   }
   uint32_t inc = sum;
@@ -218,14 +225,14 @@ __global__ void __launch_bounds__(kScanThreads)
   uint32_t run = excl + woff + (inc - sum);
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
-    s_items[tid * kScanItems + k] = run;
+    s_items[scan_pad(tid * kScanItems + k)] = run;
     run += v[k];
   }
   __syncthreads();
   for (int k = 0; k < kScanItems; ++k) {
     const uint32_t i = base + k * kScanThreads + tid;
     if (i < n) {
-      const uint32_t o = s_items[k * kScanThreads + tid];
+      const uint32_t o = s_items[scan_pad(k * kScanThreads + tid)];
       out[i] = o;
       if (owner) {
         const uint32_t c = in[i];
