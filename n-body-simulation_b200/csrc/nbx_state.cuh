@@ -205,7 +205,13 @@ __device__ __forceinline__ void root_frame_seg(const DevState &S, uint32_t sg) {
   G.cx = cx;
   G.cy = cy;
   G.size = size;
-  G.frame = sd_morton_frame(cx, cy, size);
+  // sd_morton_frame's binary64 steps in native FP64: the same IEEE
+  // operations, each correctly rounded, give the same bits
+  const double half = __dmul_rn(0.5, (double)size);
+  G.frame.x0 = (uint64_t)__double_as_longlong(__dsub_rn((double)cx, half));
+  G.frame.y0 = (uint64_t)__double_as_longlong(__dsub_rn((double)cy, half));
+  G.frame.scale = size > 0.0f ? (uint64_t)__double_as_longlong(__ddiv_rn(4294967296.0, (double)size))
+                              : 0ull;
   // clamp guard: bodies beyond the upload's coordinate limit (NaN-safe)
   const float lim = __uint_as_float(S.counters[kCtrCoordLimit]);
   const float reach = fmaxf(fmaxf(fabsf(minX), fabsf(maxX)), fmaxf(fabsf(minY), fabsf(maxY)));
