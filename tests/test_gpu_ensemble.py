@@ -118,3 +118,32 @@ def test_plain_walk_shapes(nbx, oracle, threads, pairs):
     assert same_bits(g, base.download())
     sim.close()
     base.close()
+
+
+def test_ensemble_step_io(nbx):
+    """The host-body step of a many-instance handle (force ranges that cut
+    across instances, each range's records copied while later ranges
+    compute) equals upload + step + download, bit for bit."""
+    import torch
+
+    sizes = nbx.ensemble_sizes(16, 5000, 40000)
+    bodies = nbx.ensemble_bodies(sizes)
+    n = int(np.sum(sizes))
+    assert n >= 2 * 65536  # more than one force range
+    ref = nbx.Handle(sizes, theta=0.5)
+    cur = bodies.copy()
+    expect = []
+    for _ in range(3):
+        ref.upload(cur)
+        ref.step(1)
+        cur = ref.download()
+        expect.append(cur)
+    ref.close()
+    pinned = torch.empty(n * 36, dtype=torch.uint8, pin_memory=True)
+    hb = pinned.numpy().view(nbx.BODY_DTYPE)
+    hb[:] = bodies
+    ens = nbx.Handle(sizes, theta=0.5)
+    for k in range(3):
+        ens.step_io_ptr(pinned.data_ptr(), pinned.data_ptr(), n)
+        assert same_bits(hb, expect[k]), k
+    ens.close()
