@@ -633,10 +633,21 @@ def run_b200(args):
                             force_blocks=tuned["force_blocks"],
                             force_block=tuned["force_block"], leaf_pairs=tuned["leaf_pairs"])
     inter_steps = np.empty((args.steps, 2), np.float64)
+    # the replay also checks the forces every 100 steps (and after the last)
+    # against the FP64 direct sum on the same 4096 sampled bodies (by id)
+    check_ids = np.random.default_rng(12345).choice(n, 4096, replace=False)
+    force_checks = []
     for k in range(args.steps):
         replay.step(1)
         c = replay.interactions()
         inter_steps[k] = c["far"], c["near"]
+        if (k + 1) % 100 == 0 or k + 1 == args.steps:
+            cur = replay.download()
+            where = np.empty(n, np.int64)
+            where[cur["id"]] = np.arange(n)
+            st, _ = replay.force_error(where[check_ids].astype(np.uint32))
+            force_checks.append({"step": k + 1, "p50": st["median"], "p99": st["p99"],
+                                 "max": st["max"]})
     replay_same = replay.download().tobytes() == s.tobytes()
     replay.close()
     inter = {"far": inter_steps[:, 0].mean(), "near": inter_steps[:, 1].mean()}
@@ -762,7 +773,8 @@ def run_b200(args):
                     "pass, gather, build; peak of measured (MEASURED_PEAKS.json "
                     "hbm_gbs)"},
         "force_error_fp64": {"p50": err_stats["median"], "p99": err_stats["p99"],
-                             "max": err_stats["max"], "samples": 4096},
+                             "max": err_stats["max"], "samples": 4096,
+                             "every_100_steps": force_checks},
         "interactions_per_s": (inter["far"] + inter["near"]) * 1e3 / ms,
         "gpu_launches": kernels_per_step * args.steps,
         "autotune": {k: tuned[k] for k in ("force_block", "leaf_pairs", "force_blocks",
