@@ -2127,8 +2127,9 @@ int nbx_autotune(nbx_handle *h, int allowLeaf, uint32_t steps, nbx_params *best,
     for (int threads : blockShapes)
       for (int pairs : leafWidths) {
         // grids: one warp per 32 bodies, or a half, one or two full SMs'
-        // worth of resident blocks per SM
-        const int perSm = 2048 / (threads > 0 ? threads : 256);
+        // worth of resident blocks per SM (the paired walk's launch bounds
+        // hold 1536 threads per SM, the single-body walk's 2048)
+        const int perSm = (pairs ? 1536 : 2048) / (threads > 0 ? threads : 256);
         for (int grid : {0, sms * perSm / 2, sms * perSm, sms * perSm * 2})
           trials.push_back({leaf, threads, pairs, grid});
       }

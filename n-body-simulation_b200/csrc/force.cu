@@ -456,11 +456,17 @@ __device__ __forceinline__ void forces_walk(
 // overflow, takes the clamped walk instead.  Launch bounds: a full SM of
 // kBlock-thread blocks (2048 threads: at most 32 registers) for every walk
 // but the learned correction's, whose MMA fragments keep it at 3 blocks of
-// 256.  kBlock and kPairs vary only for the default plain walk (the
-// autotuner's block shape and leaf width).
+// 256, and the default plain walk's: 1536 threads per SM (40 registers),
+// 1% faster than 2048 at 32 registers and identical in results.  kBlock
+// and kPairs vary only for the default plain walk (the autotuner's block
+// shape and leaf width).
 template <bool kExact, bool kCount = false, int kCorr = 0, bool kClamp = true,
           int kBlock = kForceBlock, bool kPairs = true>
-__global__ void __launch_bounds__(kBlock, kCorr == 1 ? 3 : 2048 / kBlock)
+__global__ void __launch_bounds__(kBlock, kCorr == 1 ? 3
+                                          : (kPairs && !kExact && !kCount && kCorr == 0 &&
+                                                     !kClamp
+                                                 ? 1536 / kBlock
+                                                 : 2048 / kBlock))
     k_forces(DevState S, float tSq, float eSq,
              unsigned long long *counts = nullptr,
              const MlpDev *__restrict__ mlp = nullptr, float bandSq = 0.0f,
