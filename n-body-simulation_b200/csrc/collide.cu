@@ -781,8 +781,6 @@ __global__ void __launch_bounds__(kBlock) k_zero_ranges(ZeroRanges z) {
 
 } // namespace
 
-// Host-side sequencing of the collision phase (no host synchronisation).
-
 // What a step's phases expect cleared, in one launch: the collision
 // counters (units, unit claims, small-large pairs, long runs of both
 // sorts), both sorts' digit rows, tile counters and look-back words (the
@@ -815,6 +813,7 @@ void launch_step_zero(cudaStream_t s, const DevState &S, ScanScratch &scan, Sort
   k_zero_ranges<<<grid_for(big / 4 + 1), kBlock, 0, s>>>(z);
 }
 
+// Host-side sequencing of the collision phase (no host synchronisation).
 void launch_integrate(cudaStream_t s, const DevState &S, bool integrate,
                       bool collide) {
   k_integrate_boxes<<<grid_for(S.n), kBlock, 0, s>>>(S, integrate ? 1 : 0,
