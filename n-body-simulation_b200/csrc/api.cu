@@ -22,8 +22,8 @@
 namespace nbx {
 void launch_integrate(cudaStream_t s, const DevState &S, bool integrate,
                       bool collide);
-void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
-                    SortScratch &sort);
+void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan, SortScratch &sort,
+                    const SideStream *side);
 void launch_bounds(cudaStream_t s, const DevState &S);
 void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
                   SortScratch &sort, bool moments);
@@ -253,6 +253,7 @@ struct nbx_handle {
   nbx_body *ioOut = nullptr;   // the host buffer the io graphs write
   bool ioCapture = false;
   cudaStream_t ioStream[kIoChunks] = {};
+  SideStream side; // a step's independent branch (collide: chain entries)
   cudaEvent_t ioFork = nullptr;
   cudaEvent_t ioDone[kIoChunks] = {};
   bool uploaded = false;
@@ -546,7 +547,7 @@ DevState enqueue_step(nbx_handle *h, cudaStream_t s, DevState S) {
   launch_step_zero(s, S, h->scan, h->sort, S.collisions != 0);
   launch_integrate(s, S, true, S.collisions != 0);
   mark(s, "integrate");
-  if (S.collisions) launch_collide(s, S, h->scan, h->sort);
+  if (S.collisions) launch_collide(s, S, h->scan, h->sort, &h->side);
   if (h->params.force_law == 1) {
     S = launch_naive_gather(s, S);
     mark(s, "naive.gather");
@@ -814,6 +815,9 @@ int nbx_create(const nbx_params *p, uint32_t num, const uint32_t *sizes,
   if (P.device >= 0) e = cudaSetDevice(P.device);
   if (e == cudaSuccess) e = cudaGetDevice(&h->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side.stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->side.fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->side.join, cudaEventDisableTiming);
   int rc = e == cudaSuccess ? allocate(h) : cuda_fail(h, e, "stream");
   if (rc != NBX_OK) {
     std::fprintf(stderr, "nbx_create: %s\n", h->lastError.c_str());
@@ -846,6 +850,9 @@ int nbx_destroy(nbx_handle *h) {
   if (h->hWord) cudaFreeHost(h->hWord);
   if (h->dPartial) cudaFree(h->dPartial);
   if (h->dTargets) cudaFree(h->dTargets);
+  if (h->side.fork) cudaEventDestroy(h->side.fork);
+  if (h->side.join) cudaEventDestroy(h->side.join);
+  if (h->side.stream) cudaStreamDestroy(h->side.stream);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return NBX_OK;
@@ -1434,7 +1441,7 @@ int nbx_phase(nbx_handle *h, int phase) {
   case NBX_PHASE_COLLIDE:
     launch_step_zero(s, S, h->scan, h->sort, true);
     launch_integrate(s, S, false, true);
-    launch_collide(s, S, h->scan, h->sort);
+    launch_collide(s, S, h->scan, h->sort, &h->side);
     h->collideValid = true;
     break;
   case NBX_PHASE_BUILD:

@@ -88,24 +88,6 @@ __global__ void k_seg_keys(DevState S, const uint32_t *__restrict__ vals,
     keys[i] = S.segOf[vals[i]];
 }
 
-// Permute the state into Morton order (the 7 gathers of
-// CudaQuadTree.cu:408-414, fused) and write the {x, y, m} traversal array.
-__global__ void __launch_bounds__(kBlock)
-    k_gather(DevState S, const uint32_t *__restrict__ perm) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n;
-       i += gridDim.x * blockDim.x) {
-    const uint32_t p = perm[i];
-    const float4 v = S.pv[p];
-    const float2 m = S.mr[p];
-    S.pv2[i] = v;
-    S.mr2[i] = m;
-    S.id2[i] = S.id[p];
-    S.xym[i] = make_float4(v.x, v.y, m.x, 0.0f);
-    S.perm[i] = p;
-    S.sortedCodes[i] = S.codes[p];
-  }
-}
-
 // ------------------------------------------------------------ tree build
 
 // Splitting nodes that start at body i: depths [lo, hi].
@@ -474,36 +456,57 @@ __global__ void __launch_bounds__(kBlock) k_upward(DevState S) {
 // This replaces the breadth-first arrays on the step path; those are built
 // only when asked for (launch_bfs_tree).
 
-// Nodes starting at each body (splitCount) and the depth of the first one
-// (splitLo).  hi_j = min(lcp(j, j+L), 31) (-1 when j+L leaves the
-// instance) is formed once per body into shared memory, then each body
-// takes the maximum over its L+1 windows.
+// Permute the state into Morton order (the 7 gathers of
+// CudaQuadTree.cu:408-414, fused), write the {x, y, m} traversal array and,
+// from the same sorted codes staged in shared memory, the traversal records
+// that start at each body: their count (splitCount) and the depth of the
+// first (splitLo).  hi_j = min(lcp(j, j+L), 31) (-1 when j+L leaves the
+// instance) is formed once per body, then each body takes the maximum over
+// its L+1 windows.  Each block takes 256 consecutive bodies and stages the
+// codes of bodies [b0 - L, b0 + 256 + L) through the permutation, so the
+// counts need no pass after the gather.
 constexpr int kMaxLeafCap = 64; // nbx_params leaf_capacity bound
-__global__ void __launch_bounds__(kBlock) k_trav_counts(DevState S) {
+__global__ void __launch_bounds__(kBlock)
+    k_gather_counts(DevState S, const uint32_t *__restrict__ perm) {
+  __shared__ uint64_t sC[kBlock + 2 * kMaxLeafCap];
   __shared__ int8_t sHi[kBlock + kMaxLeafCap];
-  const uint64_t *c = S.sortedCodes;
+  const uint32_t n = S.n;
   const uint32_t L = (uint32_t)S.leafCapacity;
-  for (uint32_t b0 = blockIdx.x * kBlock; b0 < S.n; b0 += gridDim.x * kBlock) {
-    // windows j in [b0 - L, b0 + kBlock)
+  for (uint32_t b0 = blockIdx.x * kBlock; b0 < n; b0 += gridDim.x * kBlock) {
     const uint32_t jBase = b0 >= L ? b0 - L : 0u;
-    const uint32_t span = b0 + kBlock - jBase;
+    const uint32_t cEnd = min(n, b0 + kBlock + L); // codes [jBase, cEnd)
     __syncthreads();
-    for (uint32_t t = threadIdx.x; t < span; t += kBlock) {
+    for (uint32_t t = threadIdx.x; t < cEnd - jBase; t += kBlock)
+      sC[t] = S.codes[perm[jBase + t]];
+    const uint32_t i = b0 + threadIdx.x;
+    if (i < n) {
+      const uint32_t p = perm[i];
+      const float4 v = S.pv[p];
+      const float2 m = S.mr[p];
+      S.pv2[i] = v;
+      S.mr2[i] = m;
+      S.id2[i] = S.id[p];
+      S.xym[i] = make_float4(v.x, v.y, m.x, 0.0f);
+      S.perm[i] = p;
+    }
+    __syncthreads();
+    if (i < n) S.sortedCodes[i] = sC[i - jBase];
+    // windows j in [jBase, b0 + kBlock)
+    for (uint32_t t = threadIdx.x; t < b0 + kBlock - jBase; t += kBlock) {
       const uint32_t j = jBase + t;
       int hi = -1;
-      if (j < S.n) {
+      if (j < n) {
         const SegDev &G = S.seg[S.segOf[j]];
         if ((uint64_t)j + L < (uint64_t)G.start + G.count)
-          hi = min(lcp_digits(c[j], c[j + L]), kMaxDepth - 1);
+          hi = min(lcp_digits(sC[t], sC[t + L]), kMaxDepth - 1);
       }
       sHi[t] = (int8_t)hi;
     }
     __syncthreads();
-    const uint32_t i = b0 + threadIdx.x;
-    if (i >= S.n) continue;
+    if (i >= n) continue;
     const SegDev &G = S.seg[S.segOf[i]];
     const uint32_t s0 = G.start;
-    const int lo = (i == s0) ? 0 : lcp_digits(c[i - 1], c[i]) + 1;
+    const int lo = (i == s0) ? 0 : lcp_digits(sC[i - 1 - jBase], sC[i - jBase]) + 1;
     int w = -1;
     for (uint32_t j = i >= s0 + L ? i - L : s0; j <= i; ++j) w = max(w, (int)sHi[j - jBase]);
     const int leaf = w + 1;
@@ -781,7 +784,7 @@ void launch_build(cudaStream_t s, DevState &S, ScanScratch &scan,
     const int segBits = S.nseg <= 256 ? 8 : 16;
     buf = radix_sort_u32(s, sort, n, nullptr, 0, segBits, false, false, S.status);
   }
-  k_gather<<<grid_for(n), kBlock, 0, s>>>(S, sort.vals[buf]);
+  k_gather_counts<<<grid_for(n), kBlock, 0, s>>>(S, sort.vals[buf]);
   mark(s, "build.gather");
   // swap the double-buffered state: the host mirrors this swap
   DevState T = S;
@@ -803,7 +806,7 @@ void launch_trav_tree(cudaStream_t s, const DevState &S, ScanScratch &scan, bool
   // per-record scratch in arrays only the breadth-first build uses
   uint32_t *owner = reinterpret_cast<uint32_t *>(S.start);
   uint4 *kids = reinterpret_cast<uint4 *>(S.moments);
-  k_trav_counts<<<grid_for(n), kBlock, 0, s>>>(S);
+  // the records per body (splitCount, splitLo) came with the gather
   // the scan also writes each record's first body (owner)
   exclusive_scan_u32(s, S.splitCount, S.splitStart, n, nullptr, &S.counters[6],
                      scan, S.status, owner, S.nodeCapacity, 3);

@@ -821,7 +821,7 @@ void launch_integrate(cudaStream_t s, const DevState &S, bool integrate,
 }
 
 void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
-                    SortScratch &sort) {
+                    SortScratch &sort, const SideStream *side) {
   const uint32_t n = S.n;
   // grid buckets and large lists
   exclusive_scan_u32(s, S.bucketCount, S.bucketStart, S.nBuckets + 1, nullptr,
@@ -841,6 +841,14 @@ void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
   k_partners_fill<<<grid_for(n), kBlock, 0, s>>>(S, keys32(sort, 0), unitHist);
   k_sort_large<<<64, kBlock, 0, s>>>(S, keys32(sort, 0), unitHist);
   mark(s, "collide.fill");
+  // the pairs' chain entries (k_twins) need only the sorted lists: they
+  // run beside the units' sort, on the side stream when there is one
+  if (side) {
+    cudaEventRecord(side->fork, s);
+    cudaStreamWaitEvent(side->stream, side->fork, 0);
+    k_twins<<<grid_for(n), kBlock, 0, side->stream>>>(S);
+    cudaEventRecord(side->join, side->stream);
+  }
   // units in before() order: a stable sort of all bodies' coarse keys
   // (value = index), then each run of equal coarse keys in exact minX order;
   // the first counters[1] entries are the units
@@ -850,7 +858,8 @@ void launch_collide(cudaStream_t s, DevState &S, ScanScratch &scan,
                  n / 16 + 64, S.status, true);
   mark(s, "collide.units");
   // ordered resolution
-  k_twins<<<grid_for(n), kBlock, 0, s>>>(S);
+  if (side) cudaStreamWaitEvent(s, side->join, 0);
+  else k_twins<<<grid_for(n), kBlock, 0, s>>>(S);
   k_resolve<<<148 * 8, kBlock, 0, s>>>(S, sort.vals[buf]);
   mark(s, "collide.resolve");
 }

@@ -70,6 +70,14 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return m;
 }
 
+// A second stream for a phase's independent branch: the branch waits on
+// `fork` recorded on the main stream and records `join` for the main stream
+// to wait on (in a captured step graph: two parallel branches).
+struct SideStream {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+
 // Optional phase markers: when a profiling step is running on this thread
 // (nbx_profile_step), launch sequences record an event after each stage.
 struct PhaseMarks {
